@@ -1,0 +1,216 @@
+/*
+ * pybrown_b200 -- C ABI of the B200 (sm_100a) hydrodynamics library.
+ *
+ * Two tiers:
+ *
+ *  1. Reference ABI.  The exact symbols, signatures and argument meanings of
+ *     pyBrown's native library libpyBrown (src/bdsim/clib/diff_tensor.c,
+ *     src/bdsim/clib/bead.c), as bound by ctypes in src/bdsim/pyBrown/diffusion.py
+ *     and src/bdsim/pyBrown/bead.py.  Host pointers, FP64, caller-owned
+ *     buffers.  Each call copies its inputs to the GPU, runs the sm_100a
+ *     kernels and copies the result back.  Like the reference these return
+ *     void (check_overlaps returns its flag); a failure is reported on stderr
+ *     and through pbg_last_error().
+ *
+ *  2. Device-resident API (pbg_*).  Device pointers, an explicit cudaStream_t,
+ *     int status returns (PBG_OK or a negative PBG_ERR_* code).  A pbg_system
+ *     handle owns the per-system tensors (D, B, Mff, Rff, R, positions) in HBM
+ *     and advances Brownian / Stokesian dynamics without host round trips.
+ *
+ * No torch types appear here; Python binds this with ctypes.
+ */
+#ifndef PYBROWN_B200_H
+#define PYBROWN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PBG_API __attribute__((visibility("default")))
+#else
+#define PBG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define PBG_OK 0
+#define PBG_ERR_CUDA -1       /* a CUDA runtime call failed */
+#define PBG_ERR_ARG -2        /* invalid argument */
+#define PBG_ERR_NOT_SPD -3    /* a Cholesky pivot was not positive */
+#define PBG_ERR_ATTEMPTS -4   /* max_move_attempts exceeded (box.py:248,347) */
+#define PBG_ERR_NOISE -5      /* the device noise pool ran out; step rolled back */
+#define PBG_ERR_NOMEM -6      /* device allocation failed */
+#define PBG_ERR_BARRIER -7    /* a bounded device-wide wait gave up */
+#define PBG_ERR_NAN -8        /* a non-finite value was produced */
+#define PBG_ERR_STATE -9      /* call out of order (e.g. step before set_state) */
+
+/* Message of the last error recorded on the calling thread ("" if none). */
+PBG_API const char *pbg_last_error(void);
+/* ABI version: major * 10000 + minor * 100 + patch. */
+PBG_API int pbg_version(void);
+
+/* ============================================================= Tier 1 ==== */
+/* Reference ABI, drop-in replacements for libpyBrown's exports.            */
+
+/* diff_tensor.c:73 -- free-space RPY mobility; caller passes a zeroed 9N^2 M. */
+PBG_API void RPY_M_matrix(double *as, double *pointers, int number_of_beads, double *M_matrix);
+
+/* diff_tensor.c:170 -- RPY mobility under Smith's Ewald summation. */
+PBG_API void RPY_Smith_M_matrix(double *as, double *pointers, double box_length, double alpha,
+                        int m_max, int n_max, int number_of_beads, double *M_matrix);
+
+/* diff_tensor.c:270 -- Jeffrey-Onishi two-body resistance, 18 components. */
+PBG_API void JO_2B_R_matrix(double ai, double aj, double rx, double ry, double rz, double *R_matrix);
+
+/* diff_tensor.c:346 -- lubrication correction, accumulated (+=) into a 9N^2 buffer. */
+PBG_API void JO_R_lubrication_correction_matrix(double *as, double *pointers, int number_of_beads,
+                                        double cutoff_distance, int cichocki_correction,
+                                        double *correction_matrix);
+
+/* bead.c:27 -- minimum-image pair vectors, N x N x 3. */
+PBG_API void pointer_pbc_matrix(double *positions, int number_of_beads, double box_length, double *pointers);
+
+/* bead.c:99 -- mobile/immobile pair vectors, N_mob x N_immob x 3. */
+PBG_API void pointer_immobile_pbc_matrix(double *positions_mobile, double *positions_immobile,
+                                 int number_of_mobile, int number_of_immobile,
+                                 double box_length, double *pointers);
+
+/* bead.c:169 -- 1 if any non-bonded pair overlaps, else 0. */
+PBG_API int check_overlaps(double *positions, double *as, int number_of_beads, double box_length,
+                   double overlap_treshold, int *connection_matrix);
+
+/* ============================================================= Tier 2 ==== */
+
+/* ---- stateless device kernels (device pointers, stream-ordered) -------- */
+/* Matrices are row-major with leading dimension ld (elements).  Results are
+ * multiplied by `scale` on store, which is how the callers fold in the
+ * kBT*1e19/eta (D) or 1e19/eta (Mff) factors of box.py:498-522. */
+
+/* Pair vectors (bead.c:27-95) from device positions: rij is N*N*3. */
+PBG_API int pbg_dev_pointer_matrix(const double *pos, int n_beads, double box_length, double *rij,
+                           void *stream);
+
+/* Free-space RPY (diff_tensor.c:73-166) from positions, minimum image in L. */
+PBG_API int pbg_dev_rpy_matrix(const double *pos, const double *radii, int n_beads, double box_length,
+                       double scale, double *M, int ld, void *stream);
+
+/* Smith-Ewald RPY (diff_tensor.c:170-266) from positions. precision:
+ * PBG_PREC_FP64 writes doubles to M; PBG_PREC_MIXED writes floats (M is a
+ * float*).  Scratch (phase tables) is taken from the stream-ordered pool. */
+PBG_API int pbg_dev_smith_matrix(const double *pos, const double *radii, int n_beads, double box_length,
+                         double alpha, int m_max, int n_max, double scale, int precision,
+                         void *M, int ld, void *stream);
+
+/* JO lubrication correction (diff_tensor.c:346-479) from positions, scaled
+ * by `scale` and ADDED into M (M += scale * C). */
+PBG_API int pbg_dev_lubrication_add(const double *pos, const double *radii, int n_beads,
+                            double box_length, double cutoff, int cichocki, double scale,
+                            double *M, int ld, void *stream);
+
+/* Overlap flag (bead.c:169-260) from device positions; conn may be NULL
+ * (no bonds).  The flag is written to *flag_dev (int, device). */
+PBG_API int pbg_dev_check_overlaps(const double *pos, const double *radii, int n_beads,
+                           double box_length, double threshold, const int *conn,
+                           int *flag_dev, void *stream);
+
+/* In-place lower Cholesky factor of an SPD matrix of order n (row-major,
+ * leading dimension ld >= round_up(n, 64), rows/cols n..ld-1 are used as
+ * padding).  precision selects FP64 or the mixed FP32 path (float*).
+ * info_dev (int, device) receives 0 or 1 + the index of the first
+ * non-positive pivot. */
+PBG_API int pbg_dev_cholesky(void *A, int n, int ld, int precision, int *info_dev, void *stream);
+
+/* In-place inverse of an SPD FP64 matrix via its Cholesky factor. */
+PBG_API int pbg_dev_spd_inverse(double *A, int n, int ld, int *info_dev, void *stream);
+
+/* ---- system handle -------------------------------------------------- */
+#define PBG_HI_NONE 0
+#define PBG_HI_RPY 1
+#define PBG_HI_RPY_SMITH 2
+#define PBG_HI_RPY_LUB 3
+#define PBG_HI_RPY_SMITH_LUB 4
+
+#define PBG_PREC_FP64 0
+#define PBG_PREC_MIXED 1
+
+#define PBG_SCHEME_ERMAK 0
+#define PBG_SCHEME_MIDPOINT 1
+
+/* Matrix selectors for pbg_get_matrix. */
+#define PBG_MAT_D 0
+#define PBG_MAT_B 1
+#define PBG_MAT_MFF 2
+#define PBG_MAT_RFF 3
+#define PBG_MAT_R 4
+
+typedef struct pbg_params {
+  int n_beads;
+  int hydrodynamics;       /* PBG_HI_* */
+  int precision;           /* PBG_PREC_* */
+  int propagation_scheme;  /* PBG_SCHEME_* */
+  double box_length;       /* Angstrom */
+  double kBT;              /* J (Boltzmann * T) */
+  double viscosity;        /* P */
+  double ewald_alpha;
+  int ewald_real;
+  int ewald_imag;
+  double lubrication_cutoff;
+  int cichocki_correction;
+  int check_overlaps;
+  double overlap_treshold;
+  int max_move_attempts;
+  double m_midpoint;
+} pbg_params;
+
+typedef struct pbg_system pbg_system;
+
+typedef struct pbg_step_report {
+  long long draws_consumed;   /* normals consumed from the pool */
+  long long steps_done;       /* steps fully completed */
+  int last_attempts;          /* attempts taken by the last completed step */
+  int max_attempts;           /* most attempts any step took */
+  unsigned device_errors;     /* raw device error bits */
+  int status;                 /* PBG_OK or PBG_ERR_* */
+} pbg_step_report;
+
+PBG_API int pbg_create(const pbg_params *params, pbg_system **out);
+PBG_API int pbg_destroy(pbg_system *sys);
+
+/* Copy state in (device pointers): positions N*3, radii N, connection
+ * matrix N*N int32 (NULL: no bonds), force 3N (NULL: zero). */
+PBG_API int pbg_set_state(pbg_system *sys, const double *pos, const double *radii, const int *conn,
+                  void *stream);
+PBG_API int pbg_set_force(pbg_system *sys, const double *force, void *stream);
+PBG_API int pbg_get_positions(pbg_system *sys, double *pos_out, void *stream);
+/* Copy matrix `which` (PBG_MAT_*) as a dense row-major 3N x 3N FP64 array. */
+PBG_API int pbg_get_matrix(pbg_system *sys, int which, double *out, void *stream);
+
+/* Overwrite matrix `which` from a dense row-major 3N x 3N FP64 array (restart
+ * files carry D, B, Mff, Rff and R; the mixed path rounds to FP32). */
+PBG_API int pbg_set_matrix(pbg_system *sys, int which, const double *src, void *stream);
+
+/* One Box.propagate (box.py:150-198) with host-driven attempts: the caller
+ * supplies one noise vector per attempt through the callback-free protocol
+ * pbg_step_begin / pbg_step_attempt / pbg_step_end. */
+PBG_API int pbg_step_begin(pbg_system *sys, double dt, int build_Dff, int build_Dnf, int cholesky,
+                   void *stream);
+/* Runs one attempt with noise xi (device, 3N).  *accepted_host receives 1 if
+ * the move was accepted (the call synchronises the stream). */
+PBG_API int pbg_step_attempt(pbg_system *sys, const double *xi, int *accepted_host, void *stream);
+PBG_API int pbg_step_end(pbg_system *sys, void *stream);
+
+/* Device-resident multi-step run: steps j0 .. j0+n_steps-1 with the build
+ * cadence of BD.py:177 (j % diff_freq == 0 ...).  Noise is consumed in
+ * order from `pool` (device, pool_len doubles); each attempt takes 3N.
+ * Never synchronises; read the outcome with pbg_run_report. */
+PBG_API int pbg_run(pbg_system *sys, long long j0, int n_steps, double dt, int diff_freq, int lub_freq,
+            int chol_freq, const double *pool, long long pool_len, void *stream);
+PBG_API int pbg_run_report(pbg_system *sys, pbg_step_report *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYBROWN_B200_H */

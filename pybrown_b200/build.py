@@ -1,0 +1,92 @@
+"""Build libpybrown_b200.so for sm_100a from pybrown_b200/csrc/*.cu.
+
+    python -m pybrown_b200.build [--verbose-ptxas]
+
+Objects go to pybrown_b200/_build/, the library to pybrown_b200/lib/.  nvcc
+cross-compiles, so this runs on a machine without a GPU.
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "libpybrown_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+    "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def _compile(src, verbose_ptxas):
+    obj = os.path.join(OBJ, src[:-3] + ".o")
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-dc" if False else "-c", os.path.join(CSRC, src), "-o", obj]
+    if verbose_ptxas:
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return src, obj, r.returncode, r.stdout + r.stderr
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose_ptxas=False, force=False, quiet=False):
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(ROOT, "include", "pybrown_b200.h"))
+    todo = []
+    objs = []
+    for src in sources():
+        obj = os.path.join(OBJ, src[:-3] + ".o")
+        objs.append(obj)
+        if force or verbose_ptxas or _stale(obj, [os.path.join(CSRC, src), *headers]):
+            todo.append(src)
+    failed = []
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        for src, obj, rc, out in ex.map(lambda s: _compile(s, verbose_ptxas), todo):
+            if out.strip() and (rc != 0 or verbose_ptxas or not quiet):
+                print(f"--- {src}\n{out}", file=sys.stderr)
+            if rc != 0:
+                failed.append(src)
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    if todo or not os.path.exists(LIB):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-Xlinker", "-Bsymbolic",
+               "-Xlinker", "-soname,libpybrown_b200.so", "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(verbose_ptxas=a.verbose_ptxas, force=a.force))

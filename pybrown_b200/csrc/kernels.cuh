@@ -1,0 +1,99 @@
+// Internal (C++) interfaces between the pybrown_b200 translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace pbg {
+
+// Pair index p in [0, n(n-1)/2) -> (i, j) with i > j, p = i(i-1)/2 + j.
+__device__ __forceinline__ void pair_from_linear(long long p, int& i, int& j) {
+  int ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+  while ((long long)ii * (ii - 1) / 2 > p) --ii;
+  while ((long long)(ii + 1) * ii / 2 <= p) ++ii;
+  i = ii;
+  j = (int)(p - (long long)ii * (ii - 1) / 2);
+}
+
+// Where pair vectors come from: device positions (minimum image in L) or,
+// for the reference ABI, the packed upper-triangle pair vectors the Python
+// wrappers build (diffusion.py:40,70,155): 3 doubles per pair i > j at
+// 3*((i-1) + j*(n-1) - j*(j+1)/2), value r_j - r_i.
+struct PairSource {
+  const double* pos;    // N x 3, or null
+  const double* pairs;  // packed pair vectors, or null
+  int n;
+  double L;
+};
+
+// Returns the vector the reference kernels see for pair (i > j): r_j - r_i
+// after the minimum image.
+__device__ __forceinline__ void get_pair_vector(const PairSource& s, int i, int j, double& rx,
+                                                double& ry, double& rz) {
+  if (s.pairs) {
+    const long long k = 3LL * ((i - 1) + (long long)j * (s.n - 1) - (long long)j * (j + 1) / 2);
+    rx = s.pairs[k];
+    ry = s.pairs[k + 1];
+    rz = s.pairs[k + 2];
+  } else {
+    rx = -pbg_min_image(s.pos[3 * i + 0] - s.pos[3 * j + 0], s.L);
+    ry = -pbg_min_image(s.pos[3 * i + 1] - s.pos[3 * j + 1], s.L);
+    rz = -pbg_min_image(s.pos[3 * i + 2] - s.pos[3 * j + 2], s.L);
+  }
+}
+
+// Reconstructs coordinates consistent with packed pair vectors
+// (r_0 = 0, r_i = -(r_0 - r_i) from the first column); used only for the
+// periodic phases of the reciprocal sum, which ignore lattice shifts.
+int launch_positions_from_pairs(const double* pairs, int n, double* pos, cudaStream_t st);
+
+// ---- geometry.cu ---------------------------------------------------------
+int launch_pointer_matrix(const double* pos, int n, double L, double* rij, cudaStream_t st);
+int launch_overlap(const double* pos, const double* radii, int n, double L, double thr,
+                   const int* conn, int* flag, cudaStream_t st);
+
+// ---- ewald.cu -------------------------------------------------------------
+// Reciprocal-space and real-space tables of one (alpha, m_max, n_max) set.
+struct EwaldTables {
+  double alpha = 0;
+  int m_max = -1, n_max = -1;
+  int n_real = 0;      // images with |m|_1 <= m_max (m = 0 included)
+  int n_recip = 0;     // half of the n != 0 vectors with |n|_1 <= n_max
+  double self_O[6];    // lattice sums of the self block (a-independent part)
+  double self_Q[6];
+  double* d_real = nullptr;   // n_real x 4 doubles: mx, my, mz, 0
+  double* d_recip = nullptr;  // n_recip x 8 doubles: nx, ny, nz, P, R, S, 0, 0
+  float* d_recip_f = nullptr; // same, float
+};
+
+// Returns the (cached) tables for a parameter set; they live until exit.
+int get_ewald_tables(double alpha, int m_max, int n_max, const EwaldTables** out);
+
+// Writes scale * M for the free-space (smith == false) or Smith-Ewald RPY
+// tensor of positions `pos` into M (row-major, leading dimension ld).
+// precision: PBG_PREC_FP64 (double* M) or PBG_PREC_MIXED (float* M).
+// `phase` is scratch of phase_scratch_bytes(n, tables) bytes (may be null for
+// the free-space tensor).
+size_t phase_scratch_bytes(int n, const EwaldTables* t, int precision);
+// `pos` feeds the reciprocal phases (for pair-vector input pass the
+// reconstructed coordinates of launch_positions_from_pairs).
+int launch_rpy_tensor(const PairSource& src, const double* pos, const double* radii, bool smith,
+                      const EwaldTables* t, double scale, int precision, void* M, int ld,
+                      void* phase, cudaStream_t st);
+
+// ---- lubrication.cu -------------------------------------------------------
+int launch_lubrication_add(const PairSource& src, const double* radii, double cutoff,
+                           int cichocki, double scale, double* M, int ld, cudaStream_t st);
+// Single pair, 18 components (tier-1 JO_2B_R_matrix).
+int launch_jo_pair(double ai, double aj, double rx, double ry, double rz, double* out18,
+                   cudaStream_t st);
+
+// ---- cholesky.cu ----------------------------------------------------------
+// Sets rows/cols n..ld-1 of an ld x ld matrix to the identity.
+int launch_pad_identity(void* A, int n, int ld, int precision, cudaStream_t st);
+// Workspace holds one inv(L_kk) tile per diagonal tile.
+size_t cholesky_work_bytes(int ld, int precision);
+int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st);
+size_t spd_inverse_work_bytes(int ld);
+int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st);
+
+}  // namespace pbg

@@ -1,0 +1,513 @@
+// Device-resident simulation state and one Box.propagate step
+// (src/bdsim/pyBrown/box.py:150-389, 486-556) on sm_100a.
+//
+// A pbg_system owns, in HBM, every per-system tensor of the reference's Box:
+// positions, radii, bond matrix, force, D, B and (lubrication modes) Mff, Rff,
+// R, plus the midpoint copies.  The step protocol mirrors the reference's
+// control flow one to one; the host supplies the Gaussian vector of each move
+// attempt (RandomState order) and learns whether it was accepted.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "propagate.cuh"
+#include "system.cuh"
+
+namespace pbg {
+
+namespace {
+
+template <typename T>
+__global__ void copy_lower_pad_kernel(const T* __restrict__ src, T* __restrict__ dst, int n, int ld) {
+  const long long total = (long long)ld * ld;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / ld), c = (int)(t % ld);
+    T v;
+    if (r < n && c < n) v = c <= r ? src[t] : (T)0;
+    else v = (T)(r == c ? 1 : 0);
+    dst[t] = v;
+  }
+}
+
+__global__ void scale_matrix_kernel(double* __restrict__ A, int n, int ld, double s) {
+  const long long total = (long long)n * ld;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % ld);
+    if (c < n) A[t] = s * A[t];
+  }
+}
+
+template <typename T>
+__global__ void cast_matrix_kernel(const double* __restrict__ src, T* __restrict__ dst, long long total) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    dst[t] = (T)src[t];
+}
+
+template <typename T>
+__global__ void export_matrix_kernel(const T* __restrict__ src, int n, int ld, int lower_only,
+                                     double* __restrict__ dst) {
+  const long long total = (long long)n * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    dst[t] = (lower_only && c > r) ? 0.0 : (double)src[(size_t)r * ld + c];
+  }
+}
+
+inline int grid_for(long long total) { return (int)std::min<long long>((total + 255) / 256, 148LL * 16); }
+
+}  // namespace
+
+template <typename F>
+static int sys_alloc(void** p, size_t bytes, F&&) {
+  if (bytes == 0) {
+    *p = nullptr;
+    return PBG_OK;
+  }
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    pbg_set_error_message("cudaMalloc of %zu bytes failed", bytes);
+    return PBG_ERR_NOMEM;
+  }
+  return PBG_OK;
+}
+
+#define SYS_ALLOC(ptr, bytes)                                                     \
+  do {                                                                            \
+    int _rc = sys_alloc((void**)&(ptr), (bytes), 0);                              \
+    if (_rc != PBG_OK) {                                                          \
+      destroy_system(s);                                                          \
+      return _rc;                                                                 \
+    }                                                                             \
+  } while (0)
+
+void destroy_system(pbg_system* s) {
+  if (!s) return;
+  void* ptrs[] = {s->pos,  s->pos_snap, s->radii, s->conn,  s->force, s->D,     s->B,    s->D0,
+                  s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
+                  s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
+                  s->chol_work, s->inv_work, s->dflags};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (s->hflags) cudaFreeHost(s->hflags);
+  delete s;
+}
+
+int create_system(const pbg_params* prm, pbg_system** out) {
+  if (!prm || !out) return PBG_ERR_ARG;
+  const pbg_params& p = *prm;
+  if (p.n_beads <= 0 || !(p.box_length > 0) || p.hydrodynamics < PBG_HI_NONE ||
+      p.hydrodynamics > PBG_HI_RPY_SMITH_LUB || (p.precision != PBG_PREC_FP64 && p.precision != PBG_PREC_MIXED) ||
+      (p.propagation_scheme != PBG_SCHEME_ERMAK && p.propagation_scheme != PBG_SCHEME_MIDPOINT) ||
+      (p.propagation_scheme == PBG_SCHEME_MIDPOINT && !(p.m_midpoint != 0.0))) {
+    pbg_set_error_message("invalid pbg_params");
+    return PBG_ERR_ARG;
+  }
+  pbg_system* s = new pbg_system();
+  s->p = p;
+  s->N = p.n_beads;
+  s->n = 3 * p.n_beads;
+  s->ld = pbg_round_up(s->n, PBG_TILE);
+  s->lub = p.hydrodynamics == PBG_HI_RPY_LUB || p.hydrodynamics == PBG_HI_RPY_SMITH_LUB;
+  s->smith = p.hydrodynamics == PBG_HI_RPY_SMITH || p.hydrodynamics == PBG_HI_RPY_SMITH_LUB;
+  // The lubricated resistance path runs in FP64 (the mixed path covers D and B
+  // of the far-field modes).
+  s->prec = s->lub ? PBG_PREC_FP64 : p.precision;
+  s->es = s->prec == PBG_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t N = s->N, ld = s->ld;
+  const size_t mat = ld * ld;
+  if (s->smith) {
+    int rc = get_ewald_tables(p.ewald_alpha, p.ewald_real, p.ewald_imag, &s->tables);
+    if (rc != PBG_OK) {
+      delete s;
+      return rc;
+    }
+  }
+  SYS_ALLOC(s->pos, N * 3 * sizeof(double));
+  SYS_ALLOC(s->pos_snap, N * 3 * sizeof(double));
+  SYS_ALLOC(s->radii, N * sizeof(double));
+  SYS_ALLOC(s->force, ld * sizeof(double));
+  SYS_ALLOC(s->D, mat * s->es);
+  SYS_ALLOC(s->B, mat * s->es);
+  if (p.propagation_scheme == PBG_SCHEME_MIDPOINT) SYS_ALLOC(s->D0, mat * s->es);
+  if (s->lub) {
+    SYS_ALLOC(s->Mff, mat * sizeof(double));
+    SYS_ALLOC(s->Rff, mat * sizeof(double));
+    SYS_ALLOC(s->R, mat * sizeof(double));
+    if (p.propagation_scheme == PBG_SCHEME_MIDPOINT) {
+      SYS_ALLOC(s->Mff0, mat * sizeof(double));
+      SYS_ALLOC(s->Rff0, mat * sizeof(double));
+      SYS_ALLOC(s->R0, mat * sizeof(double));
+    }
+    SYS_ALLOC(s->inv_work, spd_inverse_work_bytes(s->ld));
+  }
+  double** vecs[] = {&s->FX, &s->U, &s->BX, &s->ddet, &s->y, &s->rwork, &s->Dy, &s->drift, &s->xi};
+  for (double** v : vecs) SYS_ALLOC(*v, ld * sizeof(double));
+  if (s->smith) SYS_ALLOC(s->phase, phase_scratch_bytes(s->N, s->tables, s->prec));
+  SYS_ALLOC(s->chol_work, cholesky_work_bytes(s->ld, s->prec));
+  SYS_ALLOC(s->dflags, 8 * sizeof(int));
+  if (cudaMallocHost((void**)&s->hflags, 8 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    destroy_system(s);
+    return PBG_ERR_NOMEM;
+  }
+  // Zero every vector once so the padding entries stay zero forever.
+  for (double** v : vecs)
+    if (cudaMemset(*v, 0, ld * sizeof(double)) != cudaSuccess) {
+      destroy_system(s);
+      return PBG_ERR_CUDA;
+    }
+  cudaMemset(s->force, 0, ld * sizeof(double));
+  cudaMemset(s->dflags, 0, 8 * sizeof(int));
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    destroy_system(s);
+    return PBG_ERR_CUDA;
+  }
+  *out = s;
+  return PBG_OK;
+}
+
+int system_set_state(pbg_system* s, const double* pos, const double* radii, const int* conn, cudaStream_t st) {
+  const size_t N = s->N;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->pos, pos, N * 3 * sizeof(double), cudaMemcpyDefault, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->radii, radii, N * sizeof(double), cudaMemcpyDefault, st));
+  if (conn) {
+    if (!s->conn) {
+      if (cudaMalloc((void**)&s->conn, N * N * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return PBG_ERR_NOMEM;
+      }
+    }
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->conn, conn, N * N * sizeof(int), cudaMemcpyDefault, st));
+  } else if (s->conn) {
+    cudaFree(s->conn);
+    s->conn = nullptr;
+  }
+  s->have_state = true;
+  if (s->p.hydrodynamics == PBG_HI_NONE) return build_nohi(s, st);
+  return PBG_OK;
+}
+
+// nohi (box.py:488-490, 548-550): D = kBT 1e19 / 6 / pi / a / eta on the
+// diagonal, B = sqrt(D); kept as diagonal matrices so every other code path
+// is shared.
+int build_nohi(pbg_system* s, cudaStream_t st) {
+  std::vector<double> radii(s->N);
+  PBG_CUDA_TRY(cudaMemcpyAsync(radii.data(), s->radii, s->N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  const size_t ld = s->ld;
+  std::vector<double> D(ld * ld, 0.0), B(ld * ld, 0.0);
+  for (size_t k = 0; k < ld; ++k) {
+    if (k < (size_t)s->n) {
+      const double d = s->p.kBT * 1e19 / 6 / PBG_PI / radii[k / 3] / s->p.viscosity;
+      D[k * ld + k] = d;
+      B[k * ld + k] = std::sqrt(d);
+    } else {
+      D[k * ld + k] = B[k * ld + k] = 1.0;
+    }
+  }
+  if (s->prec == PBG_PREC_FP64) {
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->D, D.data(), ld * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->B, B.data(), ld * ld * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    std::vector<float> Df(D.begin(), D.end()), Bf(B.begin(), B.end());
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->D, Df.data(), ld * ld * sizeof(float), cudaMemcpyHostToDevice, st));
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->B, Bf.data(), ld * ld * sizeof(float), cudaMemcpyHostToDevice, st));
+  }
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  return PBG_OK;
+}
+
+static PairSource pair_source(const pbg_system* s) {
+  PairSource src;
+  src.pos = s->pos;
+  src.pairs = nullptr;
+  src.n = s->N;
+  src.L = s->p.box_length;
+  return src;
+}
+
+// box.py:486-528.
+int compute_Dff(pbg_system* s, cudaStream_t st) {
+  const pbg_params& p = s->p;
+  const bool smith = s->smith;
+  const PairSource src = pair_source(s);
+  int rc;
+  if (!s->lub) {
+    const double scale = p.kBT * 1e19 / p.viscosity;
+    rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, s->prec, s->D, s->ld, s->phase, st);
+    if (rc) return rc;
+    return launch_pad_identity(s->D, s->n, s->ld, s->prec, st);
+  }
+  const double scale = 1e19 / p.viscosity;
+  rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, PBG_PREC_FP64, s->Mff, s->ld, s->phase, st);
+  if (rc) return rc;
+  rc = launch_pad_identity(s->Mff, s->n, s->ld, PBG_PREC_FP64, st);
+  if (rc) return rc;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->Rff, s->Mff, (size_t)s->ld * s->ld * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return launch_spd_inverse(s->Rff, s->n, s->ld, s->dflags + 2, s->inv_work, st);
+}
+
+// box.py:533-541: R = C eta / 1e19 + Rff ; D = kBT inv(R).
+int compute_Dtot(pbg_system* s, cudaStream_t st) {
+  const pbg_params& p = s->p;
+  const size_t bytes = (size_t)s->ld * s->ld * sizeof(double);
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->R, s->Rff, bytes, cudaMemcpyDeviceToDevice, st));
+  int rc = launch_lubrication_add(pair_source(s), s->radii, p.lubrication_cutoff, p.cichocki_correction,
+                                  p.viscosity / 1e19, s->R, s->ld, st);
+  if (rc) return rc;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->R, bytes, cudaMemcpyDeviceToDevice, st));
+  rc = launch_spd_inverse((double*)s->D, s->n, s->ld, s->dflags + 3, s->inv_work, st);
+  if (rc) return rc;
+  scale_matrix_kernel<<<grid_for((long long)s->n * s->ld), 256, 0, st>>>((double*)s->D, s->n, s->ld, p.kBT);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+// box.py:546-556: B = chol(D), lower.
+int decompose(pbg_system* s, cudaStream_t st) {
+  if (s->p.hydrodynamics == PBG_HI_NONE) return PBG_OK;
+  const long long total = (long long)s->ld * s->ld;
+  if (s->prec == PBG_PREC_FP64)
+    copy_lower_pad_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)s->D, (double*)s->B, s->n, s->ld);
+  else
+    copy_lower_pad_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)s->D, (float*)s->B, s->n, s->ld);
+  PBG_CHECK_LAUNCH();
+  return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st);
+}
+
+static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
+  *overlap = false;
+  if (!s->p.check_overlaps) return PBG_OK;
+  int rc = launch_overlap(s->pos, s->radii, s->N, s->p.box_length, s->p.overlap_treshold, s->conn, s->dflags, st);
+  if (rc) return rc;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  *overlap = s->hflags[0] != 0;
+  return PBG_OK;
+}
+
+// Deterministic step (box.py:353-362): pos += ((dt/kBT) D @ F) * mult.
+static int deterministic_step(pbg_system* s, const void* D, double mult, cudaStream_t st) {
+  int rc = launch_gemv_scaled(D, s->ld, s->n, s->prec, s->force, s->dt / s->p.kBT, s->FX, st);
+  if (rc) return rc;
+  rc = launch_scale2(s->FX, 1.0, mult, s->n, s->FX, st);
+  if (rc) return rc;
+  return launch_translate(s->pos, s->FX, s->n, false, st);
+}
+
+// Stochastic step (box.py:366-375) from U = B @ xi: pos += (U sqrt(2 dt)) * mult.
+static int stochastic_step(pbg_system* s, double mult, cudaStream_t st) {
+  int rc = launch_scale2(s->U, std::sqrt(2 * s->dt), mult, s->n, s->BX, st);
+  if (rc) return rc;
+  return launch_translate(s->pos, s->BX, s->n, false, st);
+}
+
+int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st) {
+  if (!s->have_state) {
+    pbg_set_error_message("pbg_step_begin before pbg_set_state");
+    return PBG_ERR_STATE;
+  }
+  s->dt = dt;
+  s->build_Dff = build_Dff;
+  s->build_Dnf = build_Dnf;
+  s->cholesky = chol;
+  s->attempts = 0;
+  int rc;
+  if (s->p.hydrodynamics != PBG_HI_NONE) {
+    if (build_Dff && (rc = compute_Dff(s, st))) return rc;
+    if (s->lub && build_Dnf && (rc = compute_Dtot(s, st))) return rc;
+    if (chol && (rc = decompose(s, st))) return rc;
+  }
+  const double mult = s->p.propagation_scheme == PBG_SCHEME_MIDPOINT ? 1.0 / s->p.m_midpoint : 1.0;
+  if ((rc = deterministic_step(s, s->D, mult, st))) return rc;
+  s->in_step = true;
+  return PBG_OK;
+}
+
+// Midpoint rebuild at the predicted positions (box.py:291-304); the
+// step-start matrices move to the *0 buffers.  The midpoint Cholesky factor is
+// discarded by the reference (box.py:316), so it is not formed.
+static int midpoint_rebuild(pbg_system* s, cudaStream_t st) {
+  const size_t bytes = (size_t)s->ld * s->ld * s->es;
+  const size_t bytes64 = (size_t)s->ld * s->ld * sizeof(double);
+  std::swap(s->D, s->D0);
+  if (s->lub) {
+    std::swap(s->Mff, s->Mff0);
+    std::swap(s->Rff, s->Rff0);
+    std::swap(s->R, s->R0);
+  }
+  int rc;
+  if (s->p.hydrodynamics == PBG_HI_NONE) {
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->D0, bytes, cudaMemcpyDeviceToDevice, st));
+    return PBG_OK;
+  }
+  if (s->build_Dff) {
+    if ((rc = compute_Dff(s, st))) return rc;
+  } else {
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->D0, bytes, cudaMemcpyDeviceToDevice, st));
+    if (s->lub) {
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->Mff, s->Mff0, bytes64, cudaMemcpyDeviceToDevice, st));
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->Rff, s->Rff0, bytes64, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  if (s->lub) {
+    if (s->build_Dnf) {
+      if ((rc = compute_Dtot(s, st))) return rc;
+    } else {
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->R, s->R0, bytes64, cudaMemcpyDeviceToDevice, st));
+      if (s->build_Dff) {
+        // D keeps the step-start value when the lubrication build is skipped.
+        PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->D0, bytes, cudaMemcpyDeviceToDevice, st));
+      }
+    }
+  }
+  return PBG_OK;
+}
+
+static void midpoint_restore(pbg_system* s) {
+  std::swap(s->D, s->D0);
+  if (s->lub) {
+    std::swap(s->Mff, s->Mff0);
+    std::swap(s->Rff, s->Rff0);
+    std::swap(s->R, s->R0);
+  }
+}
+
+int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st) {
+  if (!s->in_step) {
+    pbg_set_error_message("pbg_step_attempt outside a step");
+    return PBG_ERR_STATE;
+  }
+  s->attempts++;
+  const int n = s->n;
+  int rc;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->xi, xi, n * sizeof(double), cudaMemcpyDefault, st));
+  if ((rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st))) return rc;
+  bool overlap = false;
+  if (s->p.propagation_scheme == PBG_SCHEME_ERMAK) {
+    // box.py:219-248
+    if ((rc = stochastic_step(s, 1.0, st))) return rc;
+    if ((rc = overlap_check(s, st, &overlap))) return rc;
+    if (overlap) {
+      if ((rc = stochastic_step(s, -1.0, st))) return rc;
+      *accepted = 0;
+    } else {
+      *accepted = 1;
+    }
+    return PBG_OK;
+  }
+  // Midpoint (box.py:272-347).
+  const double m = s->p.m_midpoint;
+  if ((rc = stochastic_step(s, 1.0 / m, st))) return rc;
+  if ((rc = overlap_check(s, st, &overlap))) return rc;
+  if (overlap) {
+    if ((rc = stochastic_step(s, -1.0 / m, st))) return rc;
+    *accepted = 0;
+    return PBG_OK;
+  }
+  if ((rc = midpoint_rebuild(s, st))) return rc;
+  // deterministic drift m dt / (2 kBT) (D' - D0) @ F
+  if ((rc = launch_gemv_diff(s->D, s->D0, s->ld, n, s->prec, s->force, m * s->dt / (2 * s->p.kBT), s->ddet, st)))
+    return rc;
+  // stochastic drift m/2 sqrt(2 dt) (D' inv(B0^T) - B0) @ xi = c2 (D' y - B0 xi), B0^T y = xi
+  if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) return rc;
+  if ((rc = launch_gemv_scaled(s->D, s->ld, n, s->prec, s->y, 1.0, s->Dy, st))) return rc;
+  if ((rc = launch_drift_combine(s->Dy, s->U, s->ddet, m / 2 * std::sqrt(2 * s->dt), n, s->drift, st))) return rc;
+  midpoint_restore(s);
+  if ((rc = deterministic_step(s, s->D, 1.0 - 1.0 / m, st))) return rc;
+  if ((rc = stochastic_step(s, 1.0 - 1.0 / m, st))) return rc;
+  if ((rc = launch_translate(s->pos, s->drift, n, false, st))) return rc;
+  if ((rc = overlap_check(s, st, &overlap))) return rc;
+  if (overlap) {
+    if ((rc = deterministic_step(s, s->D, -(1.0 - 1.0 / m), st))) return rc;
+    if ((rc = stochastic_step(s, -1.0, st))) return rc;
+    if ((rc = launch_translate(s->pos, s->drift, n, true, st))) return rc;
+    *accepted = 0;
+  } else {
+    *accepted = 1;
+  }
+  return PBG_OK;
+}
+
+int step_end(pbg_system* s, cudaStream_t st) {
+  if (!s->in_step) {
+    pbg_set_error_message("pbg_step_end outside a step");
+    return PBG_ERR_STATE;
+  }
+  s->in_step = false;
+  int rc = launch_wrap(s->pos, s->n, s->p.box_length, st);
+  if (rc) return rc;
+  // surface factorisation failures of this step
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (s->hflags[1] || s->hflags[2] || s->hflags[3]) {
+    pbg_set_error_message("matrix not positive definite (cholesky info %d, inverse info %d/%d)",
+                          s->hflags[1], s->hflags[2], s->hflags[3]);
+    return PBG_ERR_NOT_SPD;
+  }
+  return PBG_OK;
+}
+
+template <typename T>
+__global__ void import_matrix_kernel(const double* __restrict__ src, int n, int ld, T* __restrict__ dst) {
+  const long long total = (long long)n * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    dst[(size_t)r * ld + c] = (T)src[t];
+  }
+}
+
+int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st) {
+  void* dst = nullptr;
+  int prec = PBG_PREC_FP64;
+  switch (which) {
+    case PBG_MAT_D: dst = s->D; prec = s->prec; break;
+    case PBG_MAT_B: dst = s->B; prec = s->prec; break;
+    case PBG_MAT_MFF: dst = s->Mff; break;
+    case PBG_MAT_RFF: dst = s->Rff; break;
+    case PBG_MAT_R: dst = s->R; break;
+    default: return PBG_ERR_ARG;
+  }
+  if (!dst) return PBG_ERR_ARG;
+  int rc = launch_pad_identity(dst, s->n, s->ld, prec, st);
+  if (rc) return rc;
+  const long long total = (long long)s->n * s->n;
+  if (prec == PBG_PREC_FP64)
+    import_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>(in, s->n, s->ld, (double*)dst);
+  else
+    import_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>(in, s->n, s->ld, (float*)dst);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st) {
+  const void* src = nullptr;
+  int prec = PBG_PREC_FP64, lower = 0;
+  switch (which) {
+    case PBG_MAT_D: src = s->D; prec = s->prec; break;
+    case PBG_MAT_B: src = s->B; prec = s->prec; lower = 1; break;
+    case PBG_MAT_MFF: src = s->Mff; break;
+    case PBG_MAT_RFF: src = s->Rff; break;
+    case PBG_MAT_R: src = s->R; break;
+    default: return PBG_ERR_ARG;
+  }
+  if (!src) return PBG_ERR_ARG;
+  const long long total = (long long)s->n * s->n;
+  if (prec == PBG_PREC_FP64)
+    export_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)src, s->n, s->ld, lower, out);
+  else
+    export_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)src, s->n, s->ld, lower, out);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+}  // namespace pbg

@@ -1,0 +1,57 @@
+// The pbg_system handle (device-resident state of one simulated box).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+struct pbg_system {
+  pbg_params p{};
+  int N = 0, n = 0, ld = 0;  // beads, matrix order 3N, padded order
+  bool lub = false, smith = false;
+  int prec = PBG_PREC_FP64;  // element type of D and B
+  size_t es = 8;
+  const pbg::EwaldTables* tables = nullptr;
+
+  double* pos = nullptr;       // N x 3
+  double* pos_snap = nullptr;  // N x 3, step-start copy (device-resident runs)
+  double* radii = nullptr;     // N
+  int* conn = nullptr;         // N x N bond matrix or null
+  double* force = nullptr;     // ld (3N used)
+  void* D = nullptr;           // ld x ld, prec
+  void* B = nullptr;           // ld x ld, prec, lower factor
+  void* D0 = nullptr;          // midpoint: step-start D
+  double *Mff = nullptr, *Rff = nullptr, *R = nullptr;     // lubrication modes
+  double *Mff0 = nullptr, *Rff0 = nullptr, *R0 = nullptr;  // midpoint copies
+  double *FX = nullptr, *U = nullptr, *BX = nullptr, *ddet = nullptr, *y = nullptr;
+  double *rwork = nullptr, *Dy = nullptr, *drift = nullptr, *xi = nullptr;  // ld each
+  void* phase = nullptr;       // Ewald phase tables
+  void* chol_work = nullptr;   // inverted diagonal tiles of B
+  void* inv_work = nullptr;    // SPD inverse workspace
+  int* dflags = nullptr;       // [0] overlap, [1] cholesky info, [2] Rff info, [3] D info
+  int* hflags = nullptr;       // pinned mirror
+
+  bool have_state = false;
+  bool in_step = false;
+  double dt = 0;
+  int build_Dff = 1, build_Dnf = 1, cholesky = 1;
+  int attempts = 0;
+};
+
+namespace pbg {
+
+int create_system(const pbg_params* p, pbg_system** out);
+void destroy_system(pbg_system* s);
+int system_set_state(pbg_system* s, const double* pos, const double* radii, const int* conn, cudaStream_t st);
+int build_nohi(pbg_system* s, cudaStream_t st);
+int compute_Dff(pbg_system* s, cudaStream_t st);
+int compute_Dtot(pbg_system* s, cudaStream_t st);
+int decompose(pbg_system* s, cudaStream_t st);
+int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st);
+int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st);
+int step_end(pbg_system* s, cudaStream_t st);
+int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
+int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st);
+
+}  // namespace pbg

@@ -1,0 +1,124 @@
+"""Input and output formats (drop-in for pyBrown.input / pyBrown.output).
+
+JSON configuration with defaults and keyword validation
+(src/bdsim/pyBrown/input.py:24-109), `.str` structure files
+(input.py:113-172), `.xyz` trajectories (output.py:63-69) and pickled `.rst`
+restart files with a `.rst2` backup (output.py:72-84).  Byte formats are the
+reference's.
+"""
+import json
+import os
+import pickle
+import shutil
+import time
+
+import numpy as np
+
+from .bead import Bead
+
+
+class InputData:
+    """input.py:24-109: JSON keywords completed with defaults; missing
+    required keywords and unknown keywords raise AssertionError."""
+
+    def __init__(self, input_filename, obligatory_keywords=(), defaults=None, all_keywords=None):
+        with open(input_filename, "r") as f:
+            self.input_data = json.load(f)
+        for k, v in (defaults or {}).items():
+            if k not in self.input_data:
+                self.input_data[k] = v
+        for k in obligatory_keywords:
+            assert k in self.input_data, "Missing {} keyword in input JSON file.".format(k)
+        if all_keywords is not None:
+            for k in self.input_data:
+                assert k in all_keywords, "Unrecognized {} keyword in input JSON file.".format(k)
+
+    def __str__(self):
+        return "".join("{}: {}\n".format(k, v) for k, v in self.input_data.items())
+
+    __repr__ = __str__
+
+
+def read_str_file(input_str_filename):
+    """input.py:113-172: `sub`, `bond` and `angle` lines -> list of Bead."""
+    beads = []
+    with open(input_str_filename) as f:
+        for line in f:
+            seg = line.split()
+            if not seg:
+                continue
+            if seg[0] == "sub":
+                beads.append(Bead(coords=np.array([float(seg[i]) for i in range(3, 6)]),
+                                  hydrodynamic_radius=float(seg[6]), label=seg[1],
+                                  hard_core_radius=float(seg[8]) / 2, epsilon_LJ=float(seg[9]),
+                                  bead_id=int(seg[2])))
+            elif seg[0] == "bond":
+                id1, id2 = int(seg[1]), int(seg[2])
+                b1 = next(b for b in beads if b.bead_id == id1)
+                b1.bonded_with.append(id2)
+                b1.bonded_how[id2] = [float(seg[3]), float(seg[5])]
+            elif seg[0] == "angle":
+                id1, id2, id3 = int(seg[2]), int(seg[3]), int(seg[4])
+                b1 = next(b for b in beads if b.bead_id == id1)
+                b1.angled_with.append([id2, id3])
+                b1.angled_how[(id2, id3)] = [float(seg[5]), float(seg[6])]
+    return beads
+
+
+def write_str_file(filename, beads):
+    """Writes beads as `sub` lines (label id x y z a charge 2*lj_radius lj_energy mass)."""
+    with open(filename, "w") as f:
+        for i, b in enumerate(beads):
+            bid = b.bead_id if b.bead_id is not None else i + 1
+            f.write("sub {} {} {!r} {!r} {!r} {!r} 0 {!r} {!r} 1\n".format(
+                b.label, bid, float(b.r[0]), float(b.r[1]), float(b.r[2]), float(b.a),
+                2 * float(b.hard_core_radius), float(b.epsilon_LJ)))
+
+
+def timestamp(message, *variables):
+    date = time.asctime(time.localtime(time.time()))
+    print("{}: ".format(date) + message.format(*variables) + "\n")
+
+
+def write_to_xyz_file(xyz_file, xyz_filename, j, dt, beads):
+    """output.py:63-69."""
+    xyz_file.write("{}\n".format(len(beads)))
+    xyz_file.write("{} time [ps] {}\n".format(xyz_filename, j * dt))
+    for bead in beads:
+        xyz_file.write("{} {} {} {}\n".format(bead.label, *bead.r))
+
+
+def _file_length(filename):
+    i = -1
+    with open(filename, "r") as f:
+        for i, _ in enumerate(f):
+            pass
+    return i + 1
+
+
+def write_to_restart_file(restart_filename, index, j, box, xyz_filename, extra_output_filenames=(),
+                          extra_data=None):
+    """output.py:72-84: pickle (index, j, box, output lengths) and copy to .rst2."""
+    with open(restart_filename, "wb", buffering=0) as f:
+        pickle.dump(index, f)
+        pickle.dump(j, f)
+        pickle.dump(box, f)
+        pickle.dump(_file_length(xyz_filename), f)
+        for name in extra_output_filenames:
+            pickle.dump(_file_length(name), f)
+        if extra_data is not None:
+            pickle.dump(extra_data, f)
+    shutil.copy(restart_filename, restart_filename + "2")
+
+
+def truncate_output_file_during_restart(filename, line):
+    """output.py:44-60."""
+    tmp = filename + ".tmp"
+    with open(filename, "r") as src, open(tmp, "w") as dst:
+        for _ in range(line):
+            dst.write(src.readline())
+    with open(tmp, "r") as src, open(filename, "w") as dst:
+        for ln in src:
+            dst.write(ln)
+    if os.path.exists(tmp):
+        os.remove(tmp)
