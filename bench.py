@@ -1,0 +1,409 @@
+"""Benchmark: Brownian dynamics with hydrodynamic interactions, N=1024.
+
+Workload (the reference's headline configuration): 1024 beads, radii uniform
+in [10, 40] A, non-overlapping random positions (rejection sampling, seed 0)
+in a periodic cubic box of 1500 A; RPY tensor under Smith's Ewald summation
+(alpha = sqrt(pi), ewald_real = 2, ewald_imag = 4); Cholesky noise;
+Ermak-McCammon update, dt = 0.5 ps, T = 293.15 K, eta = 0.01005 P; overlap
+check on.  A step is one Box.propagate: Ewald build of D (3072 x 3072),
+Cholesky factor B, D F and B xi products, overlap test, update and wrap.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm times the mixed-precision path (FP32 Ewald tensor and Cholesky
+trailing updates, FP64 diagonal tiles and positions) and, for the metric's
+"vs FP64" part, the plain FP64 GPU path on the same inputs.  The reference
+arm times the reference's own CPU implementation (its C library compiled
+from source into oracle/_ref with OpenMP, NumPy LAPACK for the Cholesky)
+on the host cores.  With --gpus N > 1 every rank advances an independent
+replica (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BD steps/s, N=1024 RPY-Ewald: mixed vs FP64 (rel err ≤1e-5); serve p50/p99 ms"
+WORKLOAD = {"workload": "BD-HI N=1024 polydisperse a~U[10,40] L=1500 Smith-Ewald m=2 n=4 Ermak dt=0.5",
+            "n_beads": 1024, "box_length": 1500.0, "ewald_real": 2, "ewald_imag": 4, "dt": 0.5,
+            "seed": 0}
+
+
+def bead_config(seed, N, L, a_lo, a_hi, gap=0.0):
+    """Sequential rejection sampling: radius, then a uniform position in
+    [-L/2, L/2)^3, rejected if the minimum-image distance to any placed bead
+    is <= a_i + a_j + gap."""
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((N, 3))
+    radii = np.zeros(N)
+    k = 0
+    while k < N:
+        a = rng.uniform(a_lo, a_hi)
+        p = rng.uniform(-L / 2, L / 2, size=3)
+        if k:
+            d = pos[:k] - p
+            d -= L * np.round(d / L)
+            if np.any(np.sqrt((d * d).sum(1)) <= radii[:k] + a + gap):
+                continue
+        pos[k], radii[k] = p, a
+        k += 1
+    return pos, radii
+
+
+def box_input(precision):
+    return {"box_length": WORKLOAD["box_length"], "T": 293.15, "viscosity": 0.01005, "seed": 0,
+            "hydrodynamics": "rpy_smith", "ewald_alpha": math.sqrt(math.pi),
+            "ewald_real": WORKLOAD["ewald_real"], "ewald_imag": WORKLOAD["ewald_imag"],
+            "propagation_scheme": "ermak", "immobile_labels": [], "check_overlaps": True,
+            "overlap_treshold": 0.0, "max_move_attempts": 1000000, "external_force": [0.0, 0.0, 0.0],
+            "energy_unit": "joule", "verbose": False, "debug": False, "precision": precision,
+            "lennard_jones_6": False, "lennard_jones_12": False, "custom_interactions": False}
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        mx = float(parts[2])
+                    except ValueError:
+                        continue
+                    for nm, v in zip(names, parts[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(nm)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.remove(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- our arm
+
+class DeviceRun:
+    """Device-resident stepping through the C ABI: state, D, B and the noise
+    pool live in HBM; one pbg_step_begin / attempt / end per step."""
+
+    def __init__(self, pos, radii, precision, n_noise_steps, seed, torch):
+        from pybrown_b200 import _lib
+        from pybrown_b200.bead import Bead
+        from pybrown_b200.box import Box
+        self._lib, self.torch = _lib, torch
+        self.box = Box([Bead(p, a) for p, a in zip(pos, radii)], box_input(precision))
+        self.n = 3 * len(radii)
+        rs = np.random.RandomState(seed)
+        self.pool = torch.tensor(rs.normal(0.0, 1.0, size=(n_noise_steps + 64) * self.n), dtype=torch.float64,
+                                 device="cuda")
+        self.cursor = 0
+        self.acc = _lib.ctypes.c_int(0)
+
+    def step(self, dt):
+        _lib, h = self._lib, self.box._h
+        _lib.call("pbg_step_begin", h, dt, 1, 1, 1, None)
+        while True:
+            if (self.cursor + 1) * self.n > self.pool.numel():
+                raise RuntimeError("noise pool exhausted")
+            xi = self.pool.data_ptr() + self.cursor * self.n * 8
+            self.cursor += 1
+            _lib.call("pbg_step_attempt", h, xi, _lib.ctypes.byref(self.acc), None)
+            if self.acc.value:
+                break
+        _lib.call("pbg_step_end", h, None)
+
+    def positions(self):
+        out = np.empty(self.n)
+        self._lib.call("pbg_get_positions", self.box._h, out.ctypes.data, None)
+        self.torch.cuda.synchronize()
+        return out.reshape(-1, 3)
+
+
+def l2_flush(torch, buf):
+    buf.add_(1.0)  # 256 MiB read + write: evicts the 126 MB L2
+
+
+def timed_steps(torch, fn, steps, flush_buf):
+    """Per-step CUDA-event timing with an L2 flush between steps (outside
+    the timed interval).  Returns total milliseconds of the K steps."""
+    total = 0.0
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    for _ in range(steps):
+        l2_flush(torch, flush_buf)
+        torch.cuda.synchronize()
+        start.record()
+        fn()
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    return total
+
+
+def cholesky_kernel_timing(torch, box, reps):
+    """Average device time of the Cholesky factorisation of this step's D
+    (the dominant kernel), on the launching stream."""
+    from pybrown_b200 import _lib
+    n = 3 * len(box.beads)
+    ld = (n + 63) // 64 * 64
+    dtype = torch.float32 if box.precision == "mixed" else torch.float64
+    D = torch.tensor(box.D, dtype=dtype, device="cuda")
+    A0 = torch.zeros((ld, ld), dtype=dtype, device="cuda")
+    A0[:n, :n] = D
+    A = A0.clone()
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    prec = 1 if box.precision == "mixed" else 0
+    times = []
+    for r in range(reps + 1):
+        A.copy_(A0)
+        torch.cuda.synchronize()
+        start.record()
+        _lib.call("pbg_dev_cholesky", A.data_ptr(), n, ld, prec, info.data_ptr(), None)
+        end.record()
+        torch.cuda.synchronize()
+        if r:
+            times.append(start.elapsed_time(end))
+    return sum(times) / len(times), int(info.item())
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_reference_steps(N, steps, warmup, threads=None):
+    """The reference's CPU path: its C library (compiled from source with
+    OpenMP into oracle/_ref) for the pair vectors, Smith-Ewald tensor and
+    overlap test, NumPy LAPACK for the Cholesky, driven step by step like
+    Box.propagate.  Returns (steps/s, cores, kind, sample)."""
+    from oracle.oracle import REF_LIB, REF_OMP_LIB, ORACLE_LIB, CLib, OracleBox
+    cores = threads or len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    lib, kind = None, "reference"
+    for path in (REF_OMP_LIB, REF_LIB):
+        if os.path.exists(path):
+            lib = CLib(path)
+            break
+    if lib is None:
+        lib, kind = CLib(ORACLE_LIB), "port"
+    pos, radii = bead_config(WORKLOAD["seed"], N, WORKLOAD["box_length"], 10.0, 40.0)
+    inp = box_input("fp64")
+    box = OracleBox(pos, radii, inp, clib=lib)
+    for _ in range(warmup):
+        box.propagate(WORKLOAD["dt"])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        box.propagate(WORKLOAD["dt"])
+    dt = time.perf_counter() - t0
+    sample = (f"{steps} Box.propagate steps of the N={N} workload after {warmup} warm-up step(s); "
+              f"{os.path.basename(lib.path)} + NumPy cholesky, OMP threads={cores}")
+    return steps / dt, cores, kind, sample
+
+
+def run_ours(args, torch, dist, rank, world):
+    from pybrown_b200 import _lib
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    N = WORKLOAD["n_beads"]
+    seed = WORKLOAD["seed"] + rank  # independent replica per rank
+    pos, radii = bead_config(seed, N, WORKLOAD["box_length"], 10.0, 40.0)
+    dt = WORKLOAD["dt"]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    results = {}
+    for prec in ("mixed", "fp64"):
+        run = DeviceRun(pos, radii, prec, args.warmup + args.steps + 8, seed, torch)
+        for _ in range(args.warmup):
+            run.step(dt)
+        barrier()
+        launches0 = _lib.lib.pbg_launch_count()
+        sampler = ClockSampler(local) if prec == "mixed" else None
+        if sampler:
+            sampler.__enter__()
+        ms = timed_steps(torch, lambda: run.step(dt), args.steps, flush)
+        if sampler:
+            sampler.__exit__(None, None, None)
+        launches = _lib.lib.pbg_launch_count() - launches0
+        barrier()
+        if dist is not None:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[prec] = {"ms": ms, "launches": launches, "run": run,
+                         "clocks": sampler.summary() if sampler else None}
+
+    # mixed vs FP64 displacement error after the same warm-up + timed steps
+    p_mixed = results["mixed"]["run"].positions()
+    p_fp64 = results["fp64"]["run"].positions()
+    disp_m = p_mixed - pos
+    disp_d = p_fp64 - pos
+    L = WORKLOAD["box_length"]
+    disp_m -= L * np.round((disp_m - disp_d) / L)
+    rel_err = float(np.max(np.abs(disp_m - disp_d)) / np.max(np.abs(disp_d)))
+
+    # e2e through the public API: Box.propagate with host RandomState noise,
+    # H2D of positions and noise, D2H of positions, every step.
+    from pybrown_b200.bead import Bead
+    from pybrown_b200.box import Box
+    box = Box([Bead(p, a) for p, a in zip(pos, radii)], box_input("mixed"))
+    for _ in range(args.warmup):
+        box.propagate(dt)
+    barrier()
+    e2e_ms = timed_steps(torch, lambda: box.propagate(dt), args.steps, flush)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # dominant kernel: the Cholesky factorisation of D (3072 x 3072)
+    chol_ms, info = cholesky_kernel_timing(torch, results["mixed"]["run"].box, 3)
+    n = 3 * N
+    flops = n ** 3 / 3.0
+    peaks, peak_kind = measured_peaks()
+    achieved_tflops = flops / (chol_ms * 1e-3) / 1e12
+
+    if rank != 0:
+        return None
+    ms_step = results["mixed"]["ms"] / args.steps
+    value = world * args.steps / (results["mixed"]["ms"] * 1e-3)
+    fp64_value = world * args.steps / (results["fp64"]["ms"] * 1e-3)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        sps, cores, kind, sample = cpu_reference_steps(N, steps=2, warmup=1)
+        cpu = {"value": sps, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64 (mixed: FP32 tensor/trailing updates, FP64 diagonal tiles "
+                                       "and positions)", "data": "synthetic (seeded bead configurations)",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
+                       l2="flushed between timed steps (256 MiB write)"),
+        "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
+        "mixed_vs_fp64_displacement_rel_err": rel_err,
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
+                "h2d_bytes_per_step": 8 * 3 * N * 2 + 8 * N, "d2h_bytes_per_step": 8 * 3 * N},
+        "gpu_launches": results["mixed"]["launches"],
+        "roofline": {"kernel": "cholesky (mixed)", "bound": "tensor", "achieved": achieved_tflops,
+                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": achieved_tflops / peaks["bf16_tflops"], "traffic": None,
+                     "note": f"(3N)^3/3 = {flops:.3e} flop per factorisation in {chol_ms:.3f} ms; "
+                             f"peak is the {peak_kind} dense bf16 figure"},
+        "cpu_baseline": cpu,
+        "clocks": results["mixed"]["clocks"],
+    }
+    return line
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    N = WORKLOAD["n_beads"]
+    from oracle.oracle import REF_OMP_LIB
+    if not os.path.exists(REF_OMP_LIB):
+        return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build)"}
+    sps, cores, kind, sample = cpu_reference_steps(N, steps=args.steps, warmup=min(args.warmup, 1))
+    return {"impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / sps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bead configurations)",
+            "config": dict(WORKLOAD, parallelism="host cores"),
+            "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        line = run_ours(args, torch, dist, rank, world)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -51,6 +51,8 @@ extern "C" {
 PBG_API const char *pbg_last_error(void);
 /* ABI version: major * 10000 + minor * 100 + patch. */
 PBG_API int pbg_version(void);
+/* Number of kernels this library has launched in the process so far. */
+PBG_API long long pbg_launch_count(void);
 
 /* ============================================================= Tier 1 ==== */
 /* Reference ABI, drop-in replacements for libpyBrown's exports.            */
@@ -185,10 +187,12 @@ PBG_API int pbg_set_state(pbg_system *sys, const double *pos, const double *radi
                   void *stream);
 PBG_API int pbg_set_force(pbg_system *sys, const double *force, void *stream);
 PBG_API int pbg_get_positions(pbg_system *sys, double *pos_out, void *stream);
-/* Copy matrix `which` (PBG_MAT_*) as a dense row-major 3N x 3N FP64 array. */
+/* Copy matrix `which` (PBG_MAT_*) as a dense row-major 3N x 3N FP64 array
+ * (host or device memory; host output synchronises the stream). */
 PBG_API int pbg_get_matrix(pbg_system *sys, int which, double *out, void *stream);
 
-/* Overwrite matrix `which` from a dense row-major 3N x 3N FP64 array (restart
+/* Overwrite matrix `which` from a dense row-major 3N x 3N FP64 array in host
+ * or device memory (restart
  * files carry D, B, Mff, Rff and R; the mixed path rounds to FP32). */
 PBG_API int pbg_set_matrix(pbg_system *sys, int which, const double *src, void *stream);
 

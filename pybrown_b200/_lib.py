@@ -83,6 +83,7 @@ _SIGNATURES = {
     # tier 2
     "pbg_last_error": (ctypes.c_char_p, []),
     "pbg_version": (_i, []),
+    "pbg_launch_count": (_ll, []),
     "pbg_dev_pointer_matrix": (_i, [_vp, _i, _d, _vp, _vp]),
     "pbg_dev_rpy_matrix": (_i, [_vp, _vp, _i, _d, _d, _vp, _i, _vp]),
     "pbg_dev_smith_matrix": (_i, [_vp, _vp, _i, _d, _d, _i, _i, _d, _i, _vp, _i, _vp]),

@@ -252,11 +252,7 @@ class Box:
     def _matrix(self, name):
         n = 3 * len(self.beads)
         out = np.empty((n, n), dtype=np.float64)
-        import torch  # device staging buffer (plumbing only)
-        buf = torch.empty(n * n, dtype=torch.float64, device="cuda")
-        _lib.call("pbg_get_matrix", self._h, _lib.MAT[name], buf.data_ptr(), self._stream)
-        torch.cuda.synchronize()
-        out[:] = buf.cpu().numpy().reshape(n, n)
+        _lib.call("pbg_get_matrix", self._h, _lib.MAT[name], out.ctypes.data, self._stream)
         return out
 
     @property

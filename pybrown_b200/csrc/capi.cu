@@ -2,6 +2,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -119,6 +120,10 @@ void pbg_record_cuda_error(cudaError_t e, const char* what, const char* file, in
   g_last_error = buf;
 }
 
+static std::atomic<long long> g_launches{0};
+
+void pbg_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 void pbg_set_error_message(const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -133,6 +138,8 @@ extern "C" {
 const char* pbg_last_error(void) { return g_last_error.c_str(); }
 
 int pbg_version(void) { return 10000; }
+
+long long pbg_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 // ------------------------------------------------------------------ tier 1
 

@@ -19,6 +19,8 @@
     }                                                                             \
   } while (0)
 
+// Every kernel launch of the library is followed by this check, which also
+// counts the launch (pbg_launch_count()).
 #define PBG_CHECK_LAUNCH()                                                        \
   do {                                                                            \
     cudaError_t _e = cudaGetLastError();                                          \
@@ -26,10 +28,12 @@
       pbg_record_cuda_error(_e, "kernel launch", __FILE__, __LINE__);             \
       return PBG_ERR_CUDA;                                                        \
     }                                                                             \
+    pbg_count_launch();                                                           \
   } while (0)
 
 void pbg_record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 void pbg_set_error_message(const char* fmt, ...);
+void pbg_count_launch();
 
 // Device-side error bits (written with atomicOr into a status word).
 enum : unsigned {

@@ -466,6 +466,18 @@ __global__ void import_matrix_kernel(const double* __restrict__ src, int n, int 
   }
 }
 
+// True if `p` can be dereferenced by a kernel (device or managed memory).
+static bool device_accessible(const void* p) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Accepts host or device memory: host input is staged through a
+// stream-ordered device buffer.
 int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st) {
   void* dst = nullptr;
   int prec = PBG_PREC_FP64;
@@ -478,15 +490,29 @@ int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t s
     default: return PBG_ERR_ARG;
   }
   if (!dst) return PBG_ERR_ARG;
+  const size_t bytes = (size_t)s->n * s->n * sizeof(double);
+  const double* src = in;
+  void* stage = nullptr;
+  if (!device_accessible(in)) {
+    PBG_CUDA_TRY(cudaMallocAsync(&stage, bytes, st));
+    PBG_CUDA_TRY(cudaMemcpyAsync(stage, in, bytes, cudaMemcpyHostToDevice, st));
+    src = (const double*)stage;
+  }
   int rc = launch_pad_identity(dst, s->n, s->ld, prec, st);
-  if (rc) return rc;
-  const long long total = (long long)s->n * s->n;
-  if (prec == PBG_PREC_FP64)
-    import_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>(in, s->n, s->ld, (double*)dst);
-  else
-    import_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>(in, s->n, s->ld, (float*)dst);
-  PBG_CHECK_LAUNCH();
-  return PBG_OK;
+  if (rc == PBG_OK) {
+    const long long total = (long long)s->n * s->n;
+    if (prec == PBG_PREC_FP64)
+      import_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>(src, s->n, s->ld, (double*)dst);
+    else
+      import_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>(src, s->n, s->ld, (float*)dst);
+    if (cudaGetLastError() != cudaSuccess) rc = PBG_ERR_CUDA;
+    else pbg_count_launch();
+  }
+  if (stage) {
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    PBG_CUDA_TRY(cudaFreeAsync(stage, st));
+  }
+  return rc;
 }
 
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st) {
@@ -501,12 +527,25 @@ int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st) {
     default: return PBG_ERR_ARG;
   }
   if (!src) return PBG_ERR_ARG;
+  const size_t bytes = (size_t)s->n * s->n * sizeof(double);
+  double* dst = out;
+  void* stage = nullptr;
+  const bool host = !device_accessible(out);
+  if (host) {
+    PBG_CUDA_TRY(cudaMallocAsync(&stage, bytes, st));
+    dst = (double*)stage;
+  }
   const long long total = (long long)s->n * s->n;
   if (prec == PBG_PREC_FP64)
-    export_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)src, s->n, s->ld, lower, out);
+    export_matrix_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)src, s->n, s->ld, lower, dst);
   else
-    export_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)src, s->n, s->ld, lower, out);
+    export_matrix_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)src, s->n, s->ld, lower, dst);
   PBG_CHECK_LAUNCH();
+  if (host) {
+    PBG_CUDA_TRY(cudaMemcpyAsync(out, stage, bytes, cudaMemcpyDeviceToHost, st));
+    PBG_CUDA_TRY(cudaFreeAsync(stage, st));
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  }
   return PBG_OK;
 }
 
