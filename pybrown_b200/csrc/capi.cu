@@ -23,12 +23,35 @@ cudaStream_t legacy_stream() {
   return st;
 }
 
+// The stream-ordered pool of this process keeps freed memory instead of
+// returning it to the driver at every synchronisation (which made each
+// scratch allocation a fresh mapping); set once per device.
+void keep_pool_memory() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 // Device scratch for the reference-ABI calls, stream-ordered.
 struct DevBuf {
   void* p = nullptr;
   cudaStream_t st;
   explicit DevBuf(cudaStream_t s) : st(s) {}
   int alloc(size_t bytes) {
+    keep_pool_memory();
     if (bytes == 0) bytes = 16;
     if (cudaMallocAsync(&p, bytes, st) != cudaSuccess) {
       cudaGetLastError();
@@ -280,7 +303,7 @@ int pbg_dev_cholesky(void* A, int n, int ld, int precision, int* info_dev, void*
   if (rc) return rc;
   DevBuf work(st);
   if ((rc = work.alloc(pbg::cholesky_work_bytes(ld, precision)))) return rc;
-  return pbg::launch_cholesky_ws(A, n, ld, precision, info_dev, work.p, st);
+  return pbg::launch_cholesky_ws(A, n, ld, precision, info_dev, work.p, st, false);
 }
 
 int pbg_dev_spd_inverse(double* A, int n, int ld, int* info_dev, void* stream) {

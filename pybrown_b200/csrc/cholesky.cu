@@ -3,14 +3,10 @@
 // box.py:514,524,537, done here through the Cholesky factor).
 //
 // Storage: row-major, leading dimension ld (a multiple of 64), order padded to
-// ld with an identity block so every 64 x 64 tile is full.  Right-looking
-// tiled algorithm, one kernel per stage of each panel:
-//   potrf_diag  -- one CTA factors the diagonal tile in FP64 and forms the
-//                  inverse of the factor (for the panel solve);
-//   trsm_panel  -- one CTA per tile below it: L_ik = A_ik * inv(L_kk)^T;
-//   syrk_update -- one CTA per trailing lower tile: A_ij -= L_ik L_jk^T.
-// In the mixed precision path the matrix is FP32 and the diagonal tiles are
-// still factored and inverted in FP64.
+// ld with an identity block so every 64 x 64 tile is full.  The factorisation
+// itself is the data-flow kernel of cholesky_df.cu; this file adds the SPD
+// inverse inv(A) = inv(L)^T inv(L): block-row triangular inversion (trtri_row)
+// then the symmetric product (lauum), both tiled FP64 kernels.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -56,105 +52,6 @@ __device__ void tile_gemm_nt(const T* __restrict__ Ag, int lda, const T* __restr
     }
     __syncthreads();
   }
-}
-
-// Factor diagonal tile k in FP64; write L_kk (upper part zeroed) and
-// inv(L_kk) into invL (64 x 64, row-major).  info: 1 + first bad row.
-template <typename T>
-__global__ void __launch_bounds__(THREADS) potrf_diag_kernel(T* __restrict__ A, int ld, int k, int n,
-                                                            T* __restrict__ invL, int* __restrict__ info) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double (*L)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(smem_raw);
-  double (*X)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(smem_raw + sizeof(double) * NB * (NB + 1));
-  const int tid = threadIdx.x;
-  T* Akk = tile_ptr(A, ld, k, k);
-  for (int t = tid; t < NB * NB; t += THREADS) {
-    const int r = t / NB, c = t % NB;
-    L[r][c] = c <= r ? (double)Akk[(size_t)r * ld + c] : 0.0;
-  }
-  __syncthreads();
-  for (int j = 0; j < NB; ++j) {
-    if (tid == 0) {
-      const double d = L[j][j];
-      if (!(d > 0.0)) {
-        const int row = k * NB + j;
-        if (row < n) atomicCAS(info, 0, row + 1);
-      }
-      L[j][j] = sqrt(d);
-    }
-    __syncthreads();
-    const double d = L[j][j];
-    for (int i = j + 1 + tid; i < NB; i += THREADS) L[i][j] /= d;
-    __syncthreads();
-    // trailing lower update: elements (i, c), j < c <= i
-    const int m = NB - 1 - j;
-    for (int t = tid; t < m * m; t += THREADS) {
-      const int i = j + 1 + t / m, c = j + 1 + t % m;
-      if (c <= i) L[i][c] -= L[i][j] * L[c][j];
-    }
-    __syncthreads();
-  }
-  // inverse of the lower factor: 4 threads per column, forward substitution
-  {
-    const int col = tid / 4, part = tid % 4;
-    for (int i = 0; i < NB; ++i) {
-      double s = 0.0;
-      if (i > col)
-        for (int kk = col + part; kk < i; kk += 4) s += L[i][kk] * X[kk][col];
-      s += __shfl_xor_sync(0xffffffffu, s, 1);
-      s += __shfl_xor_sync(0xffffffffu, s, 2);
-      if (part == 0) {
-        if (i < col) X[i][col] = 0.0;
-        else if (i == col) X[i][col] = 1.0 / L[i][i];
-        else X[i][col] = -s / L[i][i];
-      }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int t = tid; t < NB * NB; t += THREADS) {
-    const int r = t / NB, c = t % NB;
-    Akk[(size_t)r * ld + c] = (T)(c <= r ? L[r][c] : 0.0);
-    invL[t] = (T)X[r][c];
-  }
-}
-
-// L_ik = A_ik * inv(L_kk)^T for tile rows i = k+1+blockIdx.x.
-template <typename T>
-__global__ void __launch_bounds__(THREADS) trsm_panel_kernel(T* __restrict__ A, int ld, int k,
-                                                            const T* __restrict__ invL) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* sA = reinterpret_cast<T*>(smem);
-  T* sB = sA + KC * (NB + 4);
-  const int i = k + 1 + blockIdx.x;
-  T acc[4][4] = {};
-  T* Aik = tile_ptr(A, ld, i, k);
-  // invL is lower triangular: row r of inv(L_kk)^T ... use B = invL (64 x 64), C = A_ik * invL^T
-  tile_gemm_nt<T>(Aik, ld, invL, NB, NB, acc, sA, sB);
-  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-  __syncthreads();
-  for (int u = 0; u < 4; ++u)
-    for (int v = 0; v < 4; ++v) Aik[(size_t)(4 * ty + u) * ld + 4 * tx + v] = acc[u][v];
-}
-
-// A_ij -= L_ik L_jk^T for all k < j <= i.
-template <typename T>
-__global__ void __launch_bounds__(THREADS) syrk_update_kernel(T* __restrict__ A, int ld, int k) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* sA = reinterpret_cast<T*>(smem);
-  T* sB = sA + KC * (NB + 4);
-  const int b = blockIdx.x;
-  int I = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-  while ((I + 1) * (I + 2) / 2 <= b) ++I;
-  while (I * (I + 1) / 2 > b) --I;
-  const int J = b - I * (I + 1) / 2;
-  const int i = k + 1 + I, j = k + 1 + J;
-  T acc[4][4] = {};
-  tile_gemm_nt<T>(tile_ptr(A, ld, i, k), ld, tile_ptr(A, ld, j, k), ld, NB, acc, sA, sB);
-  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-  T* Cij = tile_ptr(A, ld, i, j);
-  for (int u = 0; u < 4; ++u)
-    for (int v = 0; v < 4; ++v) Cij[(size_t)(4 * ty + u) * ld + 4 * tx + v] -= acc[u][v];
 }
 
 template <typename T>
@@ -282,57 +179,22 @@ int launch_pad_identity(void* A, int n, int ld, int precision, cudaStream_t st) 
   return PBG_OK;
 }
 
-// Workspace: one 64 x 64 tile for inv(L_kk) per diagonal tile (kept so the
-// SPD inverse can reuse them).
+// Workspace: [inv(L_kk) tiles, nt x 64 x 64][data-flow scratch].
 size_t cholesky_work_bytes(int ld, int precision) {
   const size_t es = precision == PBG_PREC_FP64 ? 8 : 4;
-  return (size_t)(ld / NB) * NB * NB * es;
+  return (size_t)(ld / NB) * NB * NB * es + df_work_bytes(ld);
 }
 
-constexpr size_t POTRF_SMEM = 2 * sizeof(double) * NB * (NB + 1);
-
-int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st) {
+// Factors A in place with the data-flow kernel and leaves the inverted
+// diagonal tiles of the factor at the start of `work` (used by the SPD inverse
+// and the triangular solve of the midpoint scheme).
+int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st,
+                       bool want_inverse) {
   if (ld % NB != 0 || n > ld || n < 0) return PBG_ERR_ARG;
-  static bool attr_done = false;
-  if (!attr_done) {
-    PBG_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)POTRF_SMEM));
-    PBG_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)POTRF_SMEM));
-    attr_done = true;
-  }
-  if (precision == PBG_PREC_FP64) {
-    const int nt = ld / NB;
-    double* W = (double*)work;
-    double* Ad = (double*)A;
-    const size_t smem = 2 * KC * (NB + 4) * sizeof(double);
-    PBG_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
-    for (int k = 0; k < nt; ++k) {
-      potrf_diag_kernel<double><<<1, THREADS, POTRF_SMEM, st>>>(Ad, ld, k, n, W + (size_t)k * NB * NB, info);
-      PBG_CHECK_LAUNCH();
-      const int m = nt - k - 1;
-      if (m == 0) break;
-      trsm_panel_kernel<double><<<m, THREADS, smem, st>>>(Ad, ld, k, W + (size_t)k * NB * NB);
-      PBG_CHECK_LAUNCH();
-      syrk_update_kernel<double><<<m * (m + 1) / 2, THREADS, smem, st>>>(Ad, ld, k);
-      PBG_CHECK_LAUNCH();
-    }
-    return PBG_OK;
-  }
-  const int nt = ld / NB;
-  float* W = (float*)work;
-  float* Af = (float*)A;
-  const size_t smem = 2 * KC * (NB + 4) * sizeof(float);
-  PBG_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
-  for (int k = 0; k < nt; ++k) {
-    potrf_diag_kernel<float><<<1, THREADS, POTRF_SMEM, st>>>(Af, ld, k, n, W + (size_t)k * NB * NB, info);
-    PBG_CHECK_LAUNCH();
-    const int m = nt - k - 1;
-    if (m == 0) break;
-    trsm_panel_kernel<float><<<m, THREADS, smem, st>>>(Af, ld, k, W + (size_t)k * NB * NB);
-    PBG_CHECK_LAUNCH();
-    syrk_update_kernel<float><<<m * (m + 1) / 2, THREADS, smem, st>>>(Af, ld, k);
-    PBG_CHECK_LAUNCH();
-  }
-  return PBG_OK;
+  const size_t es = precision == PBG_PREC_FP64 ? 8 : 4;
+  unsigned char* inv_tiles = static_cast<unsigned char*>(work);
+  unsigned char* df = inv_tiles + (size_t)(ld / NB) * NB * NB * es;
+  return launch_cholesky_df(A, n, ld, precision, info, want_inverse ? inv_tiles : nullptr, df, st);
 }
 
 size_t spd_inverse_work_bytes(int ld) {
@@ -344,7 +206,7 @@ int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStre
   const int nt = ld / NB;
   double* W = (double*)work;
   double* X = W + (size_t)nt * NB * NB;
-  int rc = launch_cholesky_ws(A, n, ld, PBG_PREC_FP64, info, W, st);
+  int rc = launch_cholesky_ws(A, n, ld, PBG_PREC_FP64, info, W, st, true);
   if (rc != PBG_OK) return rc;
   const size_t smem_t = (2 * KC * (NB + 4) + NB * (NB + 1)) * sizeof(double);
   PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));

@@ -90,9 +90,15 @@ int launch_jo_pair(double ai, double aj, double rx, double ry, double rz, double
 // ---- cholesky.cu ----------------------------------------------------------
 // Sets rows/cols n..ld-1 of an ld x ld matrix to the identity.
 int launch_pad_identity(void* A, int n, int ld, int precision, cudaStream_t st);
-// Workspace holds one inv(L_kk) tile per diagonal tile.
+// Workspace: inverted diagonal tiles of the factor followed by the data-flow
+// scratch (see cholesky.cu).
 size_t cholesky_work_bytes(int ld, int precision);
-int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st);
+int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st,
+                       bool want_inverse);
+// cholesky_df.cu
+size_t df_work_bytes(int ld);
+int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,
+                       cudaStream_t st);
 size_t spd_inverse_work_bytes(int ld);
 int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st);
 

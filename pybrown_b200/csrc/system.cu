@@ -280,7 +280,8 @@ int decompose(pbg_system* s, cudaStream_t st) {
   else
     copy_lower_pad_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)s->D, (float*)s->B, s->n, s->ld);
   PBG_CHECK_LAUNCH();
-  return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st);
+  return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st,
+                            s->p.propagation_scheme == PBG_SCHEME_MIDPOINT);
 }
 
 static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
@@ -448,6 +449,10 @@ int step_end(pbg_system* s, cudaStream_t st) {
   // surface factorisation failures of this step
   PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (s->hflags[1] < 0 || s->hflags[2] < 0 || s->hflags[3] < 0) {
+    pbg_set_error_message("a device-wide wait in the factorisation gave up");
+    return PBG_ERR_BARRIER;
+  }
   if (s->hflags[1] || s->hflags[2] || s->hflags[3]) {
     pbg_set_error_message("matrix not positive definite (cholesky info %d, inverse info %d/%d)",
                           s->hflags[1], s->hflags[2], s->hflags[3]);
