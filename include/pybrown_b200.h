@@ -106,6 +106,23 @@ PBG_API int pbg_dev_smith_matrix(const double *pos, const double *radii, int n_b
                          double alpha, int m_max, int n_max, double scale, int precision,
                          void *M, int ld, void *stream);
 
+/* Same result as pbg_dev_smith_matrix, for callers that cannot allocate device
+ * memory (an application whose own memory manager holds all of it, or a step
+ * loop that must not hit the device-wide synchronisation of cudaMalloc/cudaFree).
+ * No counterpart in the reference: it is an addition of this library.
+ * All scratch lives in one fixed array inside the library (about 4.3 MiB held
+ * by every GPU that loads it, until exit); nothing is allocated.  Limits:
+ * at most 4096 real-space images, 2048 reciprocal half-vectors and
+ * n_beads * (reciprocal half-vectors) * 16 bytes <= 4 MiB of phase tables
+ * (e.g. 4096 beads at ewald_imag = 4); larger inputs return PBG_ERR_ARG.
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture).  Every call reuses the same array, so calls
+ * that overlap on the GPU (different streams, or several host threads) race;
+ * the array is fully rewritten by each call before it is read. */
+PBG_API int pbg_dev_smith_matrix_noalloc(const double *pos, const double *radii, int n_beads,
+                                         double box_length, double alpha, int m_max, int n_max,
+                                         double scale, int precision, void *M, int ld, void *stream);
+
 /* JO lubrication correction (diff_tensor.c:346-479) from positions, scaled
  * by `scale` and ADDED into M (M += scale * C). */
 PBG_API int pbg_dev_lubrication_add(const double *pos, const double *radii, int n_beads,

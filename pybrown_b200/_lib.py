@@ -87,6 +87,7 @@ _SIGNATURES = {
     "pbg_dev_pointer_matrix": (_i, [_vp, _i, _d, _vp, _vp]),
     "pbg_dev_rpy_matrix": (_i, [_vp, _vp, _i, _d, _d, _vp, _i, _vp]),
     "pbg_dev_smith_matrix": (_i, [_vp, _vp, _i, _d, _d, _i, _i, _d, _i, _vp, _i, _vp]),
+    "pbg_dev_smith_matrix_noalloc": (_i, [_vp, _vp, _i, _d, _d, _i, _i, _d, _i, _vp, _i, _vp]),
     "pbg_dev_lubrication_add": (_i, [_vp, _vp, _i, _d, _d, _i, _d, _vp, _i, _vp]),
     "pbg_dev_check_overlaps": (_i, [_vp, _vp, _i, _d, _d, _vp, _vp, _vp]),
     "pbg_dev_cholesky": (_i, [_vp, _i, _i, _i, _vp, _vp]),
