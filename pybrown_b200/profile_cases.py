@@ -1,0 +1,87 @@
+"""Run one hot-path kernel on a seeded synthetic case (for profilers).
+
+    python -m pybrown_b200.profile_cases cholesky --order 768 --precision mixed
+    python -m pybrown_b200.profile_cases smith --beads 512 --precision fp64
+
+`cholesky` factors the Smith-Ewald diffusion matrix of a random bead
+configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it.
+Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
+time of one launch.
+"""
+import argparse
+import math
+
+import numpy as np
+
+
+def _config(seed, n, L, a_lo=10.0, a_hi=40.0):
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 3))
+    radii = np.zeros(n)
+    k = 0
+    while k < n:
+        a = rng.uniform(a_lo, a_hi)
+        p = rng.uniform(-L / 2, L / 2, size=3)
+        if k:
+            d = pos[:k] - p
+            d -= L * np.round(d / L)
+            if np.any(np.sqrt((d * d).sum(1)) <= radii[:k] + a):
+                continue
+        pos[k], radii[k] = p, a
+        k += 1
+    return pos, radii
+
+
+def main(argv=None):
+    import torch
+
+    from . import _lib
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("kernel", choices=("cholesky", "smith"))
+    ap.add_argument("--beads", type=int, default=256)
+    ap.add_argument("--order", type=int, default=0, help="cholesky: matrix order (default 3 x beads)")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args(argv)
+    prec = _lib.PREC[a.precision]
+    dtype = torch.float64 if prec == 0 else torch.float32
+    beads = a.order // 3 if a.order else a.beads
+    L = 1500.0 * (beads / 1024.0) ** (1.0 / 3.0)  # volume fraction of the N=1024 workload
+    pos, radii = _config(0, beads, L)
+    n = 3 * beads
+    ld = (n + 63) // 64 * 64
+    dpos = torch.tensor(pos.reshape(-1), dtype=torch.float64, device="cuda")
+    drad = torch.tensor(radii, dtype=torch.float64, device="cuda")
+    M = torch.zeros((ld, ld), dtype=dtype, device="cuda")
+    scale = 1.380649e-23 * 293.15 * 1e19 / 0.01005
+
+    def smith():
+        _lib.call("pbg_dev_smith_matrix", dpos.data_ptr(), drad.data_ptr(), beads, L, math.sqrt(math.pi), 2, 4,
+                  scale, prec, M.data_ptr(), ld, None)
+
+    smith()
+    torch.cuda.synchronize()
+    A0 = M.clone()
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def cholesky():
+        M.copy_(A0)
+        _lib.call("pbg_dev_cholesky", M.data_ptr(), n, ld, prec, info.data_ptr(), None)
+
+    fn = smith if a.kernel == "smith" else cholesky
+    fn()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(a.reps):
+        start.record()
+        fn()
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    extra = f" info={int(info.item())}" if a.kernel == "cholesky" else ""
+    print(f"{a.kernel} n={n} ({a.precision}): {total / a.reps:.3f} ms per launch{extra}")
+
+
+if __name__ == "__main__":
+    main()
