@@ -303,7 +303,7 @@ int pbg_dev_cholesky(void* A, int n, int ld, int precision, int* info_dev, void*
   if (rc) return rc;
   DevBuf work(st);
   if ((rc = work.alloc(pbg::cholesky_work_bytes(ld, precision)))) return rc;
-  return pbg::launch_cholesky_ws(A, n, ld, precision, info_dev, work.p, st, false);
+  return pbg::launch_cholesky_ws(A, n, ld, precision, info_dev, work.p, st);
 }
 
 int pbg_dev_spd_inverse(double* A, int n, int ld, int* info_dev, void* stream) {

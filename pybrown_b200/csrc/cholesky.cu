@@ -188,13 +188,12 @@ size_t cholesky_work_bytes(int ld, int precision) {
 // Factors A in place with the data-flow kernel and leaves the inverted
 // diagonal tiles of the factor at the start of `work` (used by the SPD inverse
 // and the triangular solve of the midpoint scheme).
-int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st,
-                       bool want_inverse) {
+int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st) {
   if (ld % NB != 0 || n > ld || n < 0) return PBG_ERR_ARG;
   const size_t es = precision == PBG_PREC_FP64 ? 8 : 4;
   unsigned char* inv_tiles = static_cast<unsigned char*>(work);
   unsigned char* df = inv_tiles + (size_t)(ld / NB) * NB * NB * es;
-  return launch_cholesky_df(A, n, ld, precision, info, want_inverse ? inv_tiles : nullptr, df, st);
+  return launch_cholesky_df(A, n, ld, precision, info, inv_tiles, df, st);
 }
 
 size_t spd_inverse_work_bytes(int ld) {
@@ -206,7 +205,7 @@ int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStre
   const int nt = ld / NB;
   double* W = (double*)work;
   double* X = W + (size_t)nt * NB * NB;
-  int rc = launch_cholesky_ws(A, n, ld, PBG_PREC_FP64, info, W, st, true);
+  int rc = launch_cholesky_ws(A, n, ld, PBG_PREC_FP64, info, W, st);
   if (rc != PBG_OK) return rc;
   const size_t smem_t = (2 * KC * (NB + 4) + NB * (NB + 1)) * sizeof(double);
   PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));

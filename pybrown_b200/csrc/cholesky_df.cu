@@ -1,14 +1,12 @@
 // Data-flow tiled Cholesky factorisation on sm_100a (the factor of
 // numpy.linalg.cholesky at src/bdsim/pyBrown/box.py:554).
 //
-// One persistent kernel, all CTAs co-resident (cooperative launch).  The
-// 64 x 64 tiles of the lower triangle are processed as tasks taken in a fixed
-// order from an atomic counter:
+// One persistent kernel, all CTAs co-resident (cooperative launch), one CTA
+// per SM.  The 64 x 64 tiles of the lower triangle are processed as tasks:
 //   F(k)     diagonal tile k: its last update (column k-1), then the
-//            factorisation -- 8-column panels chained by one warp in registers
-//            with rsqrt pivots, rank-8 trailing updates by the whole CTA -- and
-//            the full inverse of the factor tile (8 x 8 diagonal blocks, then
-//            the off-diagonal blocks by block distance);
+//            factorisation by 8-column panels (each 8 x 8 pivot block factored
+//            in registers with rsqrt pivots, rank-8 trailing updates on the
+//            tensor cores) and the explicit inverse inv(L_kk);
 //   S(i, k)  tile (i, k) below the diagonal: its last update, then
 //            L_ik = A_ik inv(L_kk)^T as one tensor-core tile product;
 //   U(i,j,k) trailing update A_ij -= L_ik L_jk^T (j >= k+2) on the tensor
@@ -17,16 +15,23 @@
 //            lo*hi, FP32 accumulation) in the mixed path.
 // The diagonal tiles are factored in the precision of the matrix: FP64 in
 // the FP64 path, FP32 in the mixed path.
-// Task order: F(0), S(.,0), then for each k: F(k+1), S(.,k+1), U(.,.,k) -- the
-// next panel comes before the bulk of the current trailing update (look-ahead
-// of one panel), and every task depends only on tasks earlier in the list, so
-// with all CTAs resident the lowest unfinished task can always run.
+//
+// The critical path of the factorisation is F(0), S(1,0), F(1), S(2,1), ...:
+// block 0 (the chain CTA) runs exactly that sequence and keeps what one step
+// hands to the next in shared memory (L(k, k-1) for the update of F(k) and
+// S(k+1, k); inv(L_kk) for S(k+1, k)), so the chain never waits on a round
+// trip through L2.  The other CTAs take the remaining tasks
+// in a fixed order from an atomic counter: S(., 0), then for each k the
+// solves S(i, k+1) (i >= k+3) and the updates U(., ., k), the update that
+// gates the next panel first.  Every task depends only on chain tasks and on
+// tasks earlier in the list, so with all CTAs resident the lowest unfinished
+// task can always run.
 //
 // Dependencies are tracked per tile: upd[i][j] counts applied updates,
 // fin[i][j] marks a final L tile.  Waits spin on these flags with a bounded
 // iteration count; on expiry the kernel raises an abort flag, marks info = -1
 // and every CTA returns.  Tile data written by other CTAs is read with
-// L2-coherent loads (ld.global.cg).
+// L2-coherent loads (ld.global.cg, cp.async.cg).
 #include <map>
 #include <mutex>
 #include <vector>
@@ -40,8 +45,7 @@ namespace {
 
 constexpr int NB = 64;
 constexpr int THREADS = 256;
-constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment loads)
-constexpr int LDT = NB + 1;   // FP64 factor tile row
+constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
 enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2 };
@@ -54,7 +58,7 @@ struct DFArgs {
   int* upd;      // nt * nt
   int* fin;      // nt * nt
   int* info;
-  void* leafinv; // nt * 8 * 64 (T): inverses of the 8 x 8 diagonal blocks of each L_kk
+  void* invdiag; // nt * 64 * 64 (T): inv(L_kk), row-major tiles
   unsigned* err;
 };
 
@@ -70,7 +74,8 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 #ifdef PBG_TASK_TRACE
 // Optional per-task timeline (build with -DPBG_TASK_TRACE): for task t,
-// [fetch, waits done, end] in globaltimer ns and the SM id.
+// [fetch, waits done, end] in globaltimer ns and the SM id.  The chain tasks
+// F(k), S(k+1, k) take the slots ntasks + 2k, ntasks + 2k + 1.
 __device__ long long g_task_trace[4 * 65536];
 __device__ __forceinline__ long long gtimer() {
   long long t;
@@ -157,19 +162,63 @@ __device__ __forceinline__ void stage_async(const T* g, int ld, T* s, int lds) {
   }
 }
 
+// Asynchronous copy of `count` contiguous T (count * sizeof(T) a multiple of 16).
+template <typename T>
+__device__ __forceinline__ void copy_async(const T* g, T* s, int count) {
+  constexpr int elems = 16 / (int)sizeof(T);
+  for (int t = threadIdx.x; t < count / elems; t += THREADS) cp_async16(s + t * elems, g + t * elems);
+}
+
+// 16-byte shared-memory loads of N consecutive T (p 16-byte aligned).
+template <int N>
+__device__ __forceinline__ void lds_vec(const float* p, float (&v)[N]) {
+#pragma unroll
+  for (int q = 0; q < N; q += 4) {
+    const float4 x = *reinterpret_cast<const float4*>(p + q);
+    v[q] = x.x; v[q + 1] = x.y; v[q + 2] = x.z; v[q + 3] = x.w;
+  }
+}
+template <int N>
+__device__ __forceinline__ void lds_vec(const double* p, double (&v)[N]) {
+#pragma unroll
+  for (int q = 0; q < N; q += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(p + q);
+    v[q] = x.x; v[q + 1] = x.y;
+  }
+}
+
+// Row-major copy of a 64 x 64 smem tile (rows of `lds`) to global, 16 bytes per store.
+template <typename T>
+__device__ __forceinline__ void store_tile(const T* s, int lds, T* g, int ld) {
+  constexpr int elems = 16 / (int)sizeof(T);
+  constexpr int per_row = NB / elems;
+#pragma unroll
+  for (int q = 0; q < NB * per_row / THREADS; ++q) {
+    const int t = threadIdx.x + q * THREADS;
+    const int r = t / per_row, c = (t % per_row) * elems;
+    *reinterpret_cast<float4*>(g + (size_t)r * ld + c) = *reinterpret_cast<const float4*>(s + r * lds + c);
+  }
+}
+
 // ---------------------------------------------------------------- tile GEMM
 // Accumulator layout: 16 elements per thread; warp w owns rows 16*(w/2).. and
-// columns 32*(w%2).. of the 64 x 64 tile.  acc_coord gives element e's place.
+// columns 32*(w%2).. of the 64 x 64 tile.  Each thread holds two rows
+// (row(rs), rs = 0, 1) times eight columns (col(cs), cs = 0..7); idx(rs, cs)
+// is the element's place in the accumulator array.
+__device__ __forceinline__ int acc_row(int rs) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  return 16 * (w >> 1) + 8 * rs + (lane >> 2);
+}
+__device__ __forceinline__ int acc_col(int cs) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  return 32 * (w & 1) + 8 * (cs >> 1) + 2 * (lane & 3) + (cs & 1);
+}
+
 template <typename T> struct TileMMA;
 
 template <> struct TileMMA<double> {
   // mma.m8n8k4 f64: 2 m-tiles x 4 n-tiles of 8 x 8, 2 accumulators each.
-  static __device__ __forceinline__ void coord(int e, int& r, int& c) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int mt = e >> 3, nt = (e >> 1) & 3, h = e & 1;
-    r = 16 * (w >> 1) + 8 * mt + (lane >> 2);
-    c = 32 * (w & 1) + 8 * nt + 2 * (lane & 3) + h;
-  }
+  static __device__ __forceinline__ int idx(int rs, int cs) { return rs * 8 + cs; }
   // acc -= A B^T with A, B (64 x 64, rows = output row / column, cols = k) in smem.
   static __device__ __forceinline__ void sub(const double* sA, const double* sB, double acc[16]) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -203,12 +252,7 @@ __device__ __forceinline__ unsigned to_tf32(float x) {
 
 template <> struct TileMMA<float> {
   // mma.m16n8k8 tf32: 1 m-tile of 16 x 4 n-tiles of 8, 4 accumulators each.
-  static __device__ __forceinline__ void coord(int e, int& r, int& c) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int nt = e >> 2, q = e & 3;
-    r = 16 * (w >> 1) + (lane >> 2) + 8 * (q >> 1);
-    c = 32 * (w & 1) + 8 * nt + 2 * (lane & 3) + (q & 1);
-  }
+  static __device__ __forceinline__ int idx(int rs, int cs) { return (cs >> 1) * 4 + rs * 2 + (cs & 1); }
   static __device__ __forceinline__ void sub(const float* sA, const float* sB, float acc[16]) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1), g = lane >> 2, t = lane & 3;
@@ -249,24 +293,19 @@ template <> struct TileMMA<float> {
 template <typename T>
 __device__ __forceinline__ void load_acc(const T* g, int ld, T acc[16]) {
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    int r, c;
-    TileMMA<T>::coord(e, r, c);
-    acc[e] = ldcg(g + (size_t)r * ld + c);
-  }
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) acc[TileMMA<T>::idx(rs, cs)] = ldcg(g + (size_t)acc_row(rs) * ld + acc_col(cs));
 }
 
 template <typename T>
 __device__ __forceinline__ void store_acc(T* g, int ld, const T acc[16]) {
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    int r, c;
-    TileMMA<T>::coord(e, r, c);
-    g[(size_t)r * ld + c] = acc[e];
-  }
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) g[(size_t)acc_row(rs) * ld + acc_col(cs)] = acc[TileMMA<T>::idx(rs, cs)];
 }
 
-// Apply update U(i, j, k) to acc (tile (i, j) already in acc).
 // Loads tile (i, j) into acc and applies update U(i, j, k): the two staged L
 // tiles are copied asynchronously while the accumulator loads are in flight.
 template <typename T>
@@ -281,12 +320,6 @@ __device__ __forceinline__ void load_and_update(const DFArgs& a, int i, int j, i
 }
 
 // ---------------------------------------------------------------- F(k)
-// Factor the 64 x 64 tile held in acc (already fully updated) in T arithmetic.
-// The tile stays in the accumulator registers for all eight 8-column panels:
-// the owners of panel p copy its column strip to shared memory, warp 0 factors
-// it (register chain, rsqrt pivots) and inverts its 8 x 8 diagonal block,
-// then every thread takes the final panel values back and applies the rank-8
-// update to its own trailing elements.  Two CTA barriers per panel.
 template <typename T>
 __device__ __forceinline__ T rsqrt_t(T x);
 template <>
@@ -294,259 +327,447 @@ __device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
 template <>
 __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
-constexpr int PB = 8;  // panel strip row length
+// Panel strip row length: 8 values padded so that 16-byte row loads and the
+// tensor-core fragment loads of eight different rows hit distinct banks.
+template <typename T> struct Strip { static constexpr int PB = sizeof(T) == 8 ? 10 : 12; };
 
+// Shared memory of factor_tile besides Lk and X: two panel strips
+// (alternating; reused as scratch by the inversion), the reciprocal pivots.
 template <typename T>
-__device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], unsigned char* smem) {
-  T* P = reinterpret_cast<T*>(smem);  // [64][PB] current panel strip
-  T* X = P + NB * PB;                 // [8][8][8] inverted diagonal 8 x 8 blocks
-  T* Rinv = X + 8 * 64;               // [8] 1 / L_jj of the current panel
+constexpr int factor_smem_elems() { return 2 * NB * Strip<T>::PB + NB; }
+
+// Rank-8 update acc -= Pr Pc^T of the calling warp's 16 x 32 block on the
+// tensor cores, Pr / Pc rows = the block's rows / columns of the panel strip
+// P (8 values each).  Strip rows below `lo` are read as zero, so columns
+// before the trailing part (and rows above it) are left unchanged.
+__device__ __forceinline__ void strip_update(const double* P, int lo, double acc[16]) {
+  constexpr int PB = Strip<double>::PB;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1), g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int k0 = 0; k0 < 8; k0 += 4) {
+    double a[2], b[4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const int r = m0 + 8 * mt + g;
+      a[mt] = r >= lo ? -P[r * PB + k0 + t] : 0.0;
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int c = n0 + 8 * nt + g;
+      b[nt] = c >= lo ? P[c * PB + k0 + t] : 0.0;
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        double& c0 = acc[(mt * 4 + nt) * 2];
+        double& c1 = acc[(mt * 4 + nt) * 2 + 1];
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(c0), "+d"(c1)
+                     : "d"(a[mt]), "d"(b[nt]));
+      }
+  }
+}
+
+__device__ __forceinline__ void strip_update(const float* P, int lo, float acc[16]) {
+  constexpr int PB = Strip<float>::PB;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1), g = lane >> 2, t = lane & 3;
+  unsigned ah[4], al[4];
+  {
+    const int r0 = m0 + g, r1 = m0 + g + 8;
+    const float v[4] = {r0 >= lo ? -P[r0 * PB + t] : 0.f, r1 >= lo ? -P[r1 * PB + t] : 0.f,
+                        r0 >= lo ? -P[r0 * PB + t + 4] : 0.f, r1 >= lo ? -P[r1 * PB + t + 4] : 0.f};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ah[q] = to_tf32(v[q]);
+      al[q] = to_tf32(v[q] - __uint_as_float(ah[q]));
+    }
+  }
+#pragma unroll
+  for (int nt = 0; nt < 4; ++nt) {
+    const int c = n0 + 8 * nt + g;
+    const float v0 = c >= lo ? P[c * PB + t] : 0.f;
+    const float v1 = c >= lo ? P[c * PB + t + 4] : 0.f;
+    const unsigned bh0 = to_tf32(v0), bh1 = to_tf32(v1);
+    const unsigned bl0 = to_tf32(v0 - __uint_as_float(bh0)), bl1 = to_tf32(v1 - __uint_as_float(bh1));
+    float* cc = acc + 4 * nt;
+#define PBG_TF32_MMA(A0, A1, A2, A3, B0, B1)                                                        \
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, " \
+               "{%8,%9}, {%0,%1,%2,%3};"                                                            \
+               : "+f"(cc[0]), "+f"(cc[1]), "+f"(cc[2]), "+f"(cc[3])                                 \
+               : "r"(A0), "r"(A1), "r"(A2), "r"(A3), "r"(B0), "r"(B1))
+    PBG_TF32_MMA(al[0], al[1], al[2], al[3], bh0, bh1);
+    PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bl0, bl1);
+    PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bh0, bh1);
+#undef PBG_TF32_MMA
+  }
+}
+
+// One warp's output tile D = A B of a small smem product on the tensor cores:
+// A rows with stride lda (k contiguous), B k-major rows with stride ldb, K a
+// multiple of 8.  FP64: an 8 x 8 tile (mma m8n8k4), lane holds D[g][2t + h];
+// FP32: a 16 x 8 tile (3xTF32 mma m16n8k8), lane holds D[g + 8i][2t + h].
+struct WarpTile64 {
+  static constexpr int TM = 8;
+  static __device__ __forceinline__ void mma(const double* A, int lda, const double* B, int ldb, int K, double d[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    d[0] = d[1] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const double a = A[g * lda + k0 + t], b = B[(k0 + t) * ldb + g];
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(d[0]), "+d"(d[1])
+                   : "d"(a), "d"(b));
+    }
+  }
+  // element q of the lane's part of D: row, column within the tile
+  static __device__ __forceinline__ int row(int q) { return (threadIdx.x & 31) >> 2; }
+  static __device__ __forceinline__ int col(int q) { return 2 * (threadIdx.x & 3) + (q & 1); }
+  static constexpr int NQ = 2;
+};
+
+struct WarpTile32 {
+  static constexpr int TM = 16;
+  static __device__ __forceinline__ void mma(const float* A, int lda, const float* B, int ldb, int K, float d[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    d[0] = d[1] = d[2] = d[3] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += 8) {
+      const float va[4] = {A[g * lda + k0 + t], A[(g + 8) * lda + k0 + t], A[g * lda + k0 + t + 4],
+                           A[(g + 8) * lda + k0 + t + 4]};
+      const float vb[2] = {B[(k0 + t) * ldb + g], B[(k0 + t + 4) * ldb + g]};
+      unsigned ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        ah[q] = to_tf32(va[q]);
+        al[q] = to_tf32(va[q] - __uint_as_float(ah[q]));
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        bh[q] = to_tf32(vb[q]);
+        bl[q] = to_tf32(vb[q] - __uint_as_float(bh[q]));
+      }
+#define PBG_TF32_MMA(A0, A1, A2, A3, B0, B1)                                                        \
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, " \
+               "{%8,%9}, {%0,%1,%2,%3};"                                                            \
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])                                     \
+               : "r"(A0), "r"(A1), "r"(A2), "r"(A3), "r"(B0), "r"(B1))
+      PBG_TF32_MMA(al[0], al[1], al[2], al[3], bh[0], bh[1]);
+      PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bl[0], bl[1]);
+      PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bh[0], bh[1]);
+#undef PBG_TF32_MMA
+    }
+  }
+  static __device__ __forceinline__ int row(int q) { return ((threadIdx.x & 31) >> 2) + 8 * (q >> 1); }
+  static __device__ __forceinline__ int col(int q) { return 2 * (threadIdx.x & 3) + (q & 1); }
+  static constexpr int NQ = 4;
+};
+
+template <typename T> struct WarpTileOf;
+template <> struct WarpTileOf<double> { using type = WarpTile64; };
+template <> struct WarpTileOf<float> { using type = WarpTile32; };
+
+// Inverse of the lower-triangular L_kk (in Lk, [64][LDA], zero above the
+// diagonal) into X ([64][LDA]), with Rinv[j] = 1 / L_jj and scratch Tm
+// (>= 32 x 36 T).  The eight 8 x 8 diagonal blocks are inverted by forward
+// substitution (warp b, lane c < 8 owns column c of block b); then three
+// doubling levels s = 8, 16, 32 fill the off-diagonal blocks:
+//   inv([L11 0; L21 L22]) = [X11 0; -X22 (L21 X11) X22],  X_ii = inv(L_ii),
+// each level two dependent block products: by one short dot product per
+// thread at s = 8, by warp tensor-core tiles at s = 16 and 32.
+template <typename T>
+__device__ __forceinline__ void invert_factor(const T* Lk, const T* Rinv, T* X, T* Tm) {
+  using WT = typename WarpTileOf<T>::type;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // element coordinates are recomputed where needed (keeping 32 of them live
-  // in registers made the FP64 build spill)
+  if (lane < 8) {
+    const T* D = Lk + 8 * warp * LDA + 8 * warp;
+    const T* R = Rinv + 8 * warp;
+    T x[8];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+      T sacc = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q < ii && q >= lane) sacc += D[ii * LDA + q] * x[q];
+      x[ii] = ii < lane ? T(0) : (ii == lane ? R[ii] : -sacc * R[ii]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) X[(8 * warp + ii) * LDA + 8 * warp + lane] = x[ii];
+  }
+  // blocks above the block diagonal are zero
+  for (int t = tid; t < NB * NB; t += THREADS) {
+    const int r = t >> 6, c = t & 63;
+    if ((c >> 3) > (r >> 3)) X[r * LDA + c] = T(0);
+  }
+  __syncthreads();
+  // s = 8: four 8 x 8 products per phase, one output per thread
+  {
+    const int m = tid >> 6, rr = (tid >> 3) & 7, cc = tid & 7, b0 = 16 * m;
+    T v = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v += Lk[(b0 + 8 + rr) * LDA + b0 + q] * X[(b0 + q) * LDA + b0 + cc];
+    Tm[m * 64 + rr * 8 + cc] = v;
+    __syncthreads();
+    T u = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) u += X[(b0 + 8 + rr) * LDA + b0 + 8 + q] * Tm[m * 64 + q * 8 + cc];
+    X[(b0 + 8 + rr) * LDA + b0 + cc] = -u;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int s = 16; s < NB; s *= 2) {
+    const int ldt = s + 4;                              // Tm row stride
+    const int tiles_r = s / WT::TM, tiles = (NB / (2 * s)) * tiles_r * (s / 8);
+    // Tm = L21 X11 for every 2s x 2s diagonal block
+    for (int q = warp; q < tiles; q += THREADS / 32) {
+      const int m = q / (tiles_r * (s / 8)), tr = (q / (s / 8)) % tiles_r, tc = q % (s / 8), b0 = 2 * s * m;
+      T d[4];
+      WT::mma(Lk + (b0 + s + tr * WT::TM) * LDA + b0, LDA, X + b0 * LDA + b0 + 8 * tc, LDA, s, d);
+      T* o = Tm + m * s * ldt + tr * WT::TM * ldt + 8 * tc;
+#pragma unroll
+      for (int e = 0; e < WT::NQ; ++e) o[WT::row(e) * ldt + WT::col(e)] = d[e];
+    }
+    __syncthreads();
+    // X21 = -X22 Tm
+    for (int q = warp; q < tiles; q += THREADS / 32) {
+      const int m = q / (tiles_r * (s / 8)), tr = (q / (s / 8)) % tiles_r, tc = q % (s / 8), b0 = 2 * s * m;
+      T d[4];
+      WT::mma(X + (b0 + s + tr * WT::TM) * LDA + b0 + s, LDA, Tm + m * s * ldt + 8 * tc, ldt, s, d);
+      T* o = X + (b0 + s + tr * WT::TM) * LDA + b0 + 8 * tc;
+#pragma unroll
+      for (int e = 0; e < WT::NQ; ++e) o[WT::row(e) * LDA + WT::col(e)] = -d[e];
+    }
+    __syncthreads();
+  }
+}
+
+// Factor the 64 x 64 tile held in acc (already fully updated) in T arithmetic,
+// by eight 8-column panels.  Per panel p (columns c0 = 8p .. c0+7):
+//  1. the owners copy the panel's column strip (rows >= c0) to shared memory;
+//  2. warps 0 and 1 each factor the 8 x 8 diagonal block -- every lane holds
+//     the whole block and factors it in its own registers, so the pivot chain
+//     is rsqrt -> multiply -> FMA with no shuffles -- and then each lane
+//     solves one strip row below it against the block (L_r = A_r L_pp^-T);
+//  3. every owner takes its final strip values back, and the warps whose
+//     16 x 32 block has trailing elements apply the rank-8 update on the
+//     tensor cores (strip_update).
+// Two CTA barriers per panel (the strips alternate between two buffers).
+// Then L_kk (upper triangle zeroed) goes to global memory and to Lk
+// ([64][LDA] smem), and its inverse is formed in X ([64][LDA] smem) and
+// written to the global invdiag array.  Ends with a CTA barrier.
+template <typename T>
+__device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T* fs, T* Lk, T* X) {
+  constexpr int PB = Strip<T>::PB;
+  T* Rinv = fs + 2 * NB * PB;  // [64] 1 / L_jj
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = 16 * (warp >> 1), n0 = 32 * (warp & 1);
 #pragma unroll 1
   for (int p = 0; p < 8; ++p) {
     const int c0 = 8 * p;
+    T* P = fs + (p & 1) * NB * PB;
+    // this panel's columns are the accumulator column pair (c0 - n0) / 8 of
+    // the warps with n0 <= c0 < n0 + 32
+    const bool owner = c0 >= n0 && c0 < n0 + 32;
+    const int pair = (c0 - n0) >> 3;
+    if (owner) {
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      int r, c;
-      TileMMA<T>::coord(e, r, c);
-      if (c >= c0 && c < c0 + 8 && r >= c0) P[r * PB + c - c0] = acc[e];
+      for (int q = 0; q < 4; ++q)
+        if (q == pair)
+#pragma unroll
+          for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r = acc_row(rs), cs = 2 * q + h;
+              if (r >= c0) P[r * PB + acc_col(cs) - c0] = acc[TileMMA<T>::idx(rs, cs)];
+            }
     }
     __syncthreads();
-    if (warp == 0) {
-      const int r0 = c0 + lane, r1 = c0 + 32 + lane;
-      const bool v0 = r0 < NB, v1 = r1 < NB;
-      T p0[8], p1[8];
+    if (warp < 2) {
+      // the diagonal block, in every lane (upper entries are not used)
+      T l[8][8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        p0[c] = v0 ? P[r0 * PB + c] : T(0);
-        p1[c] = v1 ? P[r1 * PB + c] : T(0);
-      }
-      // Branch-free chain: every lane takes the pivot by shuffle and computes
-      // its rsqrt; a non-positive pivot is only recorded here and reported
-      // after the panel (a branch holding an atomic inside the unrolled chain
-      // slows it several-fold).
+      for (int i = 0; i < 8; ++i) lds_vec(P + (c0 + i) * PB, l[i]);
+      const int r0 = c0 + 8 + 32 * warp + lane;
+      const bool v0 = r0 < NB;
+      T x0[8];
+      if (v0) lds_vec(P + r0 * PB, x0);
+      else
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x0[c] = T(0);
+      // right-looking 8 x 8 Cholesky; a non-positive pivot is recorded and
+      // reported after the block
       int bad = -1;
-      // 1 / L_jj goes to Rinv for the 8 x 8 block inverse
+      T rinv[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const T d = __shfl_sync(0xffffffffu, p0[j], j);
+        const T d = l[j][j];
         if (!(d > T(0)) && bad < 0) bad = j;
         const T rs = rsqrt_t<T>(d);
-        if (lane == 0) Rinv[j] = rs;
-        p0[j] = lane == j ? d * rs : (lane > j ? p0[j] * rs : p0[j]);  // L_jj = sqrt(d)
-        p1[j] *= rs;
+        rinv[j] = rs;
+        l[j][j] = d * rs;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          if (c > j) {
-            const T lc = __shfl_sync(0xffffffffu, p0[j], c);
-            if (lane >= c) p0[c] -= p0[j] * lc;
-            p1[c] -= p1[j] * lc;
-          }
-        }
+        for (int i = j + 1; i < 8; ++i) l[i][j] *= rs;
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i)
+#pragma unroll
+          for (int c = j + 1; c <= i; ++c) l[i][c] -= l[i][j] * l[c][j];
       }
-      if (lane == 0 && bad >= 0 && k * NB + c0 + bad < a.n) atomicCAS(a.info, 0, k * NB + c0 + bad + 1);
+      // the strip row below the block: x = a L_pp^-T by forward substitution
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        if (v0) P[r0 * PB + c] = c <= lane ? p0[c] : T(0);
-        if (v1) P[r1 * PB + c] = p1[c];
+      for (int j = 0; j < 8; ++j) {
+        x0[j] *= rinv[j];
+#pragma unroll
+        for (int c = j + 1; c < 8; ++c) x0[c] -= x0[j] * l[c][j];
       }
-      __syncwarp();
-      // inverse of the 8 x 8 diagonal block: lane c < 8 owns column c
-      if (lane < 8) {
-        T x[8];
+      if (v0)
 #pragma unroll
-        for (int ii = 0; ii < 8; ++ii) {
-          T sacc = 0;
+        for (int c = 0; c < 8; ++c) P[r0 * PB + c] = x0[c];
+      if (warp == 0 && lane == 0) {
 #pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (q < ii && q >= lane) sacc += P[(c0 + ii) * PB + q] * x[q];
-          x[ii] = ii < lane ? T(0) : (ii == lane ? Rinv[ii] : -sacc * Rinv[ii]);
+        for (int i = 0; i < 8; ++i) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) P[(c0 + i) * PB + c] = c <= i ? l[i][c] : T(0);
+          Rinv[c0 + i] = rinv[i];
         }
-#pragma unroll
-        for (int ii = 0; ii < 8; ++ii) X[p * 64 + ii * 8 + lane] = x[ii];
+        if (bad >= 0 && k * NB + c0 + bad < a.n) atomicCAS(a.info, 0, k * NB + c0 + bad + 1);
       }
     }
     __syncthreads();
+    // final values of this panel's strip back into the accumulators
+    if (owner) {
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      int r, c;
-      TileMMA<T>::coord(e, r, c);
-      if (c >= c0 && c < c0 + 8) {
-        if (r >= c0) acc[e] = P[r * PB + c - c0];
-      } else if (c >= c0 + 8 && r >= c) {
-        T s0 = 0, s1 = 0;
+      for (int q = 0; q < 4; ++q)
+        if (q == pair)
 #pragma unroll
-        for (int q = 0; q < 8; q += 2) {
-          s0 += P[r * PB + q] * P[c * PB + q];
-          s1 += P[r * PB + q + 1] * P[c * PB + q + 1];
-        }
-        acc[e] -= s0 + s1;
-      }
+          for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int r = acc_row(rs), cs = 2 * q + h;
+              if (r >= c0) acc[TileMMA<T>::idx(rs, cs)] = P[r * PB + acc_col(cs) - c0];
+            }
     }
-    // the next panel's strip is written only after everyone has read this one
-    __syncthreads();
+    // trailing elements (c >= c0 + 8, r >= c) exist in this warp's block?
+    const int lo = c0 + 8;
+    if (m0 + 15 >= lo && m0 + 15 >= n0 && n0 + 31 >= lo) strip_update(P, lo, acc);
+    // no barrier here: the next panel writes the other strip buffer, and the
+    // two barriers of that panel separate these reads from its next reuse
   }
   T* g = tile<T>(a, k, k);
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    int r, c;
-    TileMMA<T>::coord(e, r, c);
-    g[(size_t)r * a.ld + c] = c <= r ? acc[e] : T(0);
-  }
-  T* li = reinterpret_cast<T*>(a.leafinv) + (size_t)k * 8 * 64;
-  for (int t = tid; t < 8 * 64; t += THREADS) li[t] = X[t];
-}
-
-// ---------------------------------------------------------------- S(i, k)
-// acc holds the updated A_ik; computes L_ik = A_ik L_kk^-T in T arithmetic by
-// 8-column blocks: X_b = (A_b - sum_{b'<b} X_b' L_bb'^T) inv(L_bb)^T.
-// Row r belongs to the four threads 4r .. 4r+3 (two columns of each block),
-// so rows proceed independently with warp-level syncs only.
-constexpr int LDW = NB + 4;
-
-template <typename T>
-__device__ __forceinline__ void solve_tile(const DFArgs& a, int i, int k, const T acc[16], unsigned char* smem) {
-  T* C = reinterpret_cast<T*>(smem);  // [64][LDW] rhs, becomes X
-  T* Lk = C + NB * LDW;               // [64][LDW] L_kk
-  T* Inv = Lk + NB * LDW;             // [8][8][8]
-  T* W = Inv + 8 * 64;                // [64][9]
-  const int tid = threadIdx.x;
-  stage_async(tile<T>(a, k, k), a.ld, Lk, LDW);
-  {
-    const T* li = reinterpret_cast<const T*>(a.leafinv) + (size_t)k * 8 * 64;
-    constexpr int chunks = 8 * 64 * (int)sizeof(T) / 16;
-    constexpr int elems = 16 / (int)sizeof(T);
-    for (int t = tid; t < chunks; t += THREADS) cp_async16(Inv + t * elems, li + t * elems);
-  }
+  for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    int r, c;
-    TileMMA<T>::coord(e, r, c);
-    C[r * LDW + c] = acc[e];
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int r = tid >> 2, q2 = 2 * (tid & 3);
-  // block loop kept rolled: the kernel's code footprint matters more than
-  // the loop overhead (the persistent kernel runs every task type)
-#pragma unroll 1
-  for (int b = 0; b < 8; ++b) {
-    const int o = 8 * b;
-    T u0 = 0, u1 = 0, v0 = 0, v1 = 0;
-#pragma unroll 4
-    for (int j = 0; j < o; j += 2) {
-      const T x0 = C[r * LDW + j], x1 = C[r * LDW + j + 1];
-      u0 += x0 * Lk[(o + q2) * LDW + j];
-      v0 += x1 * Lk[(o + q2) * LDW + j + 1];
-      u1 += x0 * Lk[(o + q2 + 1) * LDW + j];
-      v1 += x1 * Lk[(o + q2 + 1) * LDW + j + 1];
+    for (int cs = 0; cs < 8; ++cs) {
+      const int r = acc_row(rs), c = acc_col(cs);
+      const T v = c <= r ? acc[TileMMA<T>::idx(rs, cs)] : T(0);
+      g[(size_t)r * a.ld + c] = v;
+      Lk[r * LDA + c] = v;
     }
-    W[r * 9 + q2] = C[r * LDW + o + q2] - (u0 + v0);
-    W[r * 9 + q2 + 1] = C[r * LDW + o + q2 + 1] - (u1 + v1);
-    __syncwarp();
-    T s0 = 0, s1 = 0;
+  __syncthreads();
+  invert_factor(Lk, Rinv, X, fs);
+  store_tile(X, LDA, reinterpret_cast<T*>(a.invdiag) + (size_t)k * NB * NB, NB);
+}
+
+// acc = -(acc + ...) helpers for S: acc = C inv(L_kk)^T with C, X in smem.
+template <typename T>
+__device__ __forceinline__ void solve_by_inverse(const T* C, const T* X, T acc[16]) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const T wq = W[r * 9 + q];
-      s0 += wq * Inv[b * 64 + q2 * 8 + q];  // inv is lower: zero above the diagonal
-      s1 += wq * Inv[b * 64 + (q2 + 1) * 8 + q];
-    }
-    C[r * LDW + o + q2] = s0;
-    C[r * LDW + o + q2 + 1] = s1;
-    __syncwarp();
-  }
-  __syncthreads();
-  T* g = tile<T>(a, i, k);
-  for (int t = tid; t < NB * NB; t += THREADS) {
-    const int rr = t >> 6, c = t & 63;
-    g[(size_t)rr * a.ld + c] = C[rr * LDW + c];
-  }
-}
-
-// Inverse of every diagonal factor tile (one CTA per tile), from L_kk and the
-// inverted 8 x 8 blocks: X_ab = -inv(L_aa) sum_{c=b}^{a-1} L_ac X_cb by block
-// distance.  Needed only by the SPD inverse and the midpoint triangular solve.
-template <typename T>
-__global__ void __launch_bounds__(THREADS) diag_inverse_kernel(const T* __restrict__ A, int ld,
-                                                               const T* __restrict__ leafinv,
-                                                               T* __restrict__ out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* L = reinterpret_cast<T*>(smem_raw);  // [64][LDT]
-  T* X = L + NB * LDT;                    // [64][LDT]
-  T* Tm = X + NB * LDT;                   // [7][8][9]
-  const int k = blockIdx.x, tid = threadIdx.x;
-  const T* g = A + (size_t)k * NB * ld + (size_t)k * NB;
-  for (int t = tid; t < NB * NB; t += THREADS) {
-    const int r = t >> 6, c = t & 63;
-    L[r * LDT + c] = g[(size_t)r * ld + c];
-    X[r * LDT + c] = T(0);
-  }
-  __syncthreads();
-  const T* li = leafinv + (size_t)k * 8 * 64;
-  for (int t = tid; t < 8 * 64; t += THREADS) {
-    const int b = t >> 6, r = (t >> 3) & 7, c = t & 7;
-    X[(8 * b + r) * LDT + 8 * b + c] = li[t];
-  }
-  __syncthreads();
-  for (int d = 1; d < 8; ++d) {
-    const int nblk = 8 - d;
-    for (int t = tid; t < nblk * 64; t += THREADS) {
-      const int b = t >> 6, r = (t >> 3) & 7, c = t & 7, aa = b + d;
-      T s0 = 0;
-      for (int q = 8 * b; q < 8 * aa; ++q) s0 += L[(8 * aa + r) * LDT + q] * X[q * LDT + 8 * b + c];
-      Tm[b * 72 + r * 9 + c] = s0;
-    }
-    __syncthreads();
-    for (int t = tid; t < nblk * 64; t += THREADS) {
-      const int b = t >> 6, r = (t >> 3) & 7, c = t & 7, aa = b + d;
-      T v = 0;
-      for (int q = 0; q <= r; ++q) v -= X[(8 * aa + r) * LDT + 8 * aa + q] * Tm[b * 72 + q * 9 + c];
-      X[(8 * aa + r) * LDT + 8 * b + c] = v;
-    }
-    __syncthreads();
-  }
-  T* o = out + (size_t)k * NB * NB;
-  for (int t = tid; t < NB * NB; t += THREADS) o[t] = X[(t >> 6) * LDT + (t & 63)];
+  for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  TileMMA<T>::sub(C, X, acc);  // acc = -C X^T
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
 }
 
 template <typename T>
-__global__ void __launch_bounds__(THREADS, 2) chol_df_kernel(DFArgs a) {
+__device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
+#pragma unroll
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) s[acc_row(rs) * LDA + acc_col(cs)] = acc[TileMMA<T>::idx(rs, cs)];
+}
+
+// Shared memory of the chain CTA (in T elements): four tiles Cp, Cn, X, sA
+// ([64][LDA] each; sA also holds L_kk during F) and the factor scratch.
+// Every piece is a multiple of 16 bytes, so each starts 16-byte aligned.
+template <typename T>
+constexpr int chain_smem_elems() { return 4 * NB * LDA + factor_smem_elems<T>(); }
+
+// The chain CTA: F(0), S(1, 0), F(1), S(2, 1), ... with L(k, k-1) and
+// inv(L_kk) kept in shared memory from one task to the next.
+template <typename T>
+__device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
+  T* Cp = reinterpret_cast<T*>(smem);  // L(k, k-1), the previous solve's result
+  T* Cn = Cp + NB * LDA;               // this step's solve input / result L(k+1, k)
+  T* X = Cn + NB * LDA;                // inv(L_kk)
+  T* sA = X + NB * LDA;                // L_kk during F(k); then staged L(k+1, k-1)
+  T* fs = sA + NB * LDA;               // factor scratch
+  const int nt = a.nt;
+  for (int k = 0; k < nt; ++k) {
+    T acc[16];
+    // F(k): A_kk after updates 0 .. k-2 (other CTAs), minus L(k,k-1) L(k,k-1)^T
+    TRACE(0, a.ntasks + 2 * k);
+    TRACE(3, a.ntasks + 2 * k);
+    if (k > 0) {
+      if (!wait_geq(a, a.upd + k * nt + k, k - 1, s_ok)) return;
+      load_acc(tile<T>(a, k, k), a.ld, acc);
+      TileMMA<T>::sub(Cp, Cp, acc);  // Cp is complete: the last solve ended with a barrier
+    } else {
+      load_acc(tile<T>(a, 0, 0), a.ld, acc);
+    }
+    TRACE(1, a.ntasks + 2 * k);
+    factor_tile<T>(a, k, acc, fs, sA, X);
+    publish(a.fin + k * nt + k, 1);
+    TRACE(2, a.ntasks + 2 * k);
+    if (k + 1 == nt) return;
+    // S(k+1, k): A(k+1,k) after updates 0 .. k-2, minus L(k+1,k-1) L(k,k-1)^T,
+    // times inv(L_kk)^T
+    TRACE(0, a.ntasks + 2 * k + 1);
+    TRACE(3, a.ntasks + 2 * k + 1);
+    if (k > 0) {
+      const int* fl[2] = {a.fin + (k + 1) * nt + k - 1, a.upd + (k + 1) * nt + k};
+      const int tg[2] = {1, k - 1};
+      if (!wait_all(a, fl, tg, 2, s_ok)) return;
+      stage_async(tile<T>(a, k + 1, k - 1), a.ld, sA, LDA);
+      load_acc(tile<T>(a, k + 1, k), a.ld, acc);
+      cp_async_wait_all();
+      __syncthreads();
+      TileMMA<T>::sub(sA, Cp, acc);
+    } else {
+      load_acc(tile<T>(a, 1, 0), a.ld, acc);
+    }
+    TRACE(1, a.ntasks + 2 * k + 1);
+    acc_to_smem(acc, Cn);
+    __syncthreads();
+    solve_by_inverse(Cn, X, acc);
+    __syncthreads();  // every warp has read Cn
+    acc_to_smem(acc, Cn);
+    store_acc(tile<T>(a, k + 1, k), a.ld, acc);
+    publish(a.fin + (k + 1) * nt + k, 1);
+    TRACE(2, a.ntasks + 2 * k + 1);
+    T* t = Cp;
+    Cp = Cn;
+    Cn = t;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_task, s_ok;
+  if (blockIdx.x == 0) {
+    run_chain<T>(a, smem, &s_ok);
+    return;
+  }
   T* sA = reinterpret_cast<T*>(smem);
   T* sB = sA + NB * LDA;
   const int nt = a.nt;
-  // Block 0 is the chain CTA: it runs, in order, every diagonal factorisation
-  // F(k) and the solve S(k+1, k) that gates F(k+1), so that code stays warm in
-  // one SM and the chain has no inter-CTA hand-off.  The other CTAs take the
-  // remaining tasks from the shared counter, in list order.
-  const bool chain = blockIdx.x == 0;
-  int chain_step = 0;
   while (true) {
-    int t, type, i, j, k;
-    if (chain) {
-      if (chain_step >= 2 * nt - 1) return;
-      const int kk = chain_step >> 1;
-      if (chain_step & 1) { type = TASK_S; i = kk + 1; j = k = kk; }
-      else { type = TASK_F; i = j = k = kk; }
-      t = a.ntasks + chain_step;  // trace slot after the shared tasks
-      ++chain_step;
-      if (threadIdx.x == 0 && ld_acquire(a.ctl + 1)) s_task = -1;
-      else if (threadIdx.x == 0) s_task = 0;
-      __syncthreads();
-      if (s_task < 0) return;
-      __syncthreads();
-    } else {
-      if (threadIdx.x == 0) s_task = ld_acquire(a.ctl + 1) ? a.ntasks : atomicAdd(a.ctl, 1);
-      __syncthreads();
-      t = s_task;
-      __syncthreads();
-      if (t >= a.ntasks) return;
-      const int4 tk = a.tasks[t];
-      type = tk.x; i = tk.y; j = tk.z; k = tk.w;
-    }
+    if (threadIdx.x == 0) s_task = ld_acquire(a.ctl + 1) ? a.ntasks : atomicAdd(a.ctl, 1);
+    __syncthreads();
+    const int t = s_task;
+    __syncthreads();
+    if (t >= a.ntasks) return;
+    const int4 tk = a.tasks[t];
+    const int type = tk.x, i = tk.y, j = tk.z, k = tk.w;
     TRACE(0, t);
     TRACE(3, t);
     T acc[16];
@@ -561,24 +782,24 @@ __global__ void __launch_bounds__(THREADS, 2) chol_df_kernel(DFArgs a) {
       publish(a.upd + i * nt + j, k + 1);
       TRACE(2, t);
     } else {
-      // F(j) (i == j) or S(i, j): the tile in column j, after its last update
+      // S(i, j), i >= j + 2: the tile after its last update, times inv(L_jj)^T
       const int col = j;
       if (col > 0) {
         const int* fl[3] = {a.fin + i * nt + col - 1, a.fin + col * nt + col - 1, a.upd + i * nt + col};
         const int tg[3] = {1, 1, col - 1};
         if (!wait_all(a, fl, tg, 3, &s_ok)) return;
-        load_and_update(a, i, col, col - 1, acc, sA, sB);
+        load_and_update(a, i, col, col - 1, acc, sA, sB);  // ends with a barrier: smem is free
       } else {
         load_acc(tile<T>(a, i, col), a.ld, acc);
       }
-      if (type == TASK_F) {
-        TRACE(1, t);
-        factor_tile<T>(a, col, acc, smem);
-      } else {
-        if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
-        TRACE(1, t);
-        solve_tile<T>(a, i, col, acc, smem);
-      }
+      if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
+      TRACE(1, t);
+      stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);
+      acc_to_smem(acc, sA);
+      cp_async_wait_all();
+      __syncthreads();
+      solve_by_inverse(sA, sB, acc);
+      store_acc(tile<T>(a, i, col), a.ld, acc);
       publish(a.fin + i * nt + col, 1);
       TRACE(2, t);
     }
@@ -589,7 +810,7 @@ __global__ void __launch_bounds__(THREADS, 2) chol_df_kernel(DFArgs a) {
 std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
-// Task list of an nt x nt tile grid (see the file comment).
+// Task list of the worker CTAs for an nt x nt tile grid (see the file comment).
 int get_task_table(int nt, const int4** out, int* count) {
   std::lock_guard<std::mutex> lk(g_task_mu);
   auto it = g_task_tables.find(nt);
@@ -609,11 +830,13 @@ int get_task_table(int nt, const int4** out, int* count) {
       for (int i = jj; i < nt; ++i) t.push_back(make_int4(TASK_U, i, jj, k));
   }
   int4* d = nullptr;
-  if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) {
-    cudaGetLastError();
-    return PBG_ERR_NOMEM;
+  if (!t.empty()) {
+    if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) {
+      cudaGetLastError();
+      return PBG_ERR_NOMEM;
+    }
+    PBG_CUDA_TRY(cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
-  PBG_CUDA_TRY(cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
   g_task_tables[nt] = std::make_pair(d, (int)t.size());
   *out = d;
   *count = (int)t.size();
@@ -622,15 +845,11 @@ int get_task_table(int nt, const int4** out, int* count) {
 
 template <typename T>
 size_t df_smem_bytes() {
-  const size_t gemm = 2 * sizeof(T) * NB * LDA;
-  const size_t fac = sizeof(T) * (NB * PB + 8 * 64 + 8);
-  const size_t sol = sizeof(T) * (2 * NB * LDW + 8 * 64 + NB * 9);
-  size_t m = gemm > fac ? gemm : fac;
-  return m > sol ? m : sol;
+  return sizeof(T) * (size_t)chain_smem_elems<T>();
 }
 
 template <typename T>
-int launch_df(T* A, int n, int ld, int* info, void* leafinv, int* ints, unsigned* err, cudaStream_t st) {
+int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned* err, cudaStream_t st) {
   const int nt = ld / NB;
   const int4* tasks = nullptr;
   int ntasks = 0;
@@ -650,7 +869,8 @@ int launch_df(T* A, int n, int ld, int* info, void* leafinv, int* ints, unsigned
       return PBG_ERR_CUDA;
     }
   }
-  int grid = num_sms * max_blocks_per_sm;
+  // one CTA per SM: the chain CTA has its SM to itself
+  int grid = num_sms;
   if (grid > ntasks + 1) grid = ntasks + 1;  // the chain CTA plus the shared tasks
   PBG_CUDA_TRY(cudaMemsetAsync(ints, 0, (3 + 2 * (size_t)nt * nt) * sizeof(int), st));
   PBG_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
@@ -665,7 +885,7 @@ int launch_df(T* A, int n, int ld, int* info, void* leafinv, int* ints, unsigned
   args.upd = ints + 3;
   args.fin = ints + 3 + nt * nt;
   args.info = info;
-  args.leafinv = leafinv;
+  args.invdiag = invdiag;
   args.err = err;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
@@ -691,35 +911,28 @@ extern "C" __attribute__((visibility("default"))) int pbg_task_trace(long long* 
 }
 #endif
 
-// Scratch of one factorisation: leaf inverses, task counter, abort flag,
-// per-tile flags, error word.
+// Scratch of one factorisation: task counter, abort flag, per-tile flags,
+// error word.
 size_t df_work_bytes(int ld) {
   const int nt = ld / NB;
-  return (size_t)nt * 8 * 64 * sizeof(double) + (3 + 2 * (size_t)nt * nt + 1) * sizeof(int) + 64;
+  return (3 + 2 * (size_t)nt * nt + 1) * sizeof(int) + 64;
 }
 
-// Factors A in place.  With invdiag non-null, the inverse of every diagonal
-// factor tile is then written there (nt x 64 x 64, precision of A).
+// Factors A in place and writes the inverse of every diagonal factor tile to
+// invdiag (nt x 64 x 64 row-major tiles, precision of A; the solves of the
+// factorisation use them, and so do the SPD inverse and the triangular solve
+// of the midpoint scheme).  Both A and invdiag start on 16-byte boundaries.
 int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,
                        cudaStream_t st) {
   const int nt = ld / NB;
-  unsigned char* w = static_cast<unsigned char*>(work);
-  void* leafinv = w;
-  int* ints = reinterpret_cast<int*>(w + (size_t)nt * 8 * 64 * sizeof(double));
-  unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 2 * (size_t)nt * nt);
-  int rc = precision == PBG_PREC_FP64 ? launch_df<double>((double*)A, n, ld, info, leafinv, ints, err, st)
-                                      : launch_df<float>((float*)A, n, ld, info, leafinv, ints, err, st);
-  if (rc != PBG_OK || !invdiag) return rc;
-  const size_t smem = (precision == PBG_PREC_FP64 ? 8 : 4) * (2 * NB * LDT + 7 * 72);
-  if (precision == PBG_PREC_FP64) {
-    PBG_CUDA_TRY(cudaFuncSetAttribute(diag_inverse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    diag_inverse_kernel<double><<<nt, THREADS, smem, st>>>((const double*)A, ld, (const double*)leafinv, (double*)invdiag);
-  } else {
-    PBG_CUDA_TRY(cudaFuncSetAttribute(diag_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    diag_inverse_kernel<float><<<nt, THREADS, smem, st>>>((const float*)A, ld, (const float*)leafinv, (float*)invdiag);
+  if (reinterpret_cast<uintptr_t>(A) % 16 != 0 || reinterpret_cast<uintptr_t>(invdiag) % 16 != 0) {
+    pbg_set_error_message("cholesky: the matrix and its workspace must start on 16-byte boundaries");
+    return PBG_ERR_ARG;
   }
-  PBG_CHECK_LAUNCH();
-  return PBG_OK;
+  int* ints = static_cast<int*>(work);
+  unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 2 * (size_t)nt * nt);
+  return precision == PBG_PREC_FP64 ? launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st)
+                                    : launch_df<float>((float*)A, n, ld, info, invdiag, ints, err, st);
 }
 
 }  // namespace pbg

@@ -93,8 +93,7 @@ int launch_pad_identity(void* A, int n, int ld, int precision, cudaStream_t st);
 // Workspace: inverted diagonal tiles of the factor followed by the data-flow
 // scratch (see cholesky.cu).
 size_t cholesky_work_bytes(int ld, int precision);
-int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st,
-                       bool want_inverse);
+int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st);
 // cholesky_df.cu
 size_t df_work_bytes(int ld);
 int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,

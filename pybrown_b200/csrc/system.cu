@@ -280,8 +280,7 @@ int decompose(pbg_system* s, cudaStream_t st) {
   else
     copy_lower_pad_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)s->D, (float*)s->B, s->n, s->ld);
   PBG_CHECK_LAUNCH();
-  return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st,
-                            s->p.propagation_scheme == PBG_SCHEME_MIDPOINT);
+  return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st);
 }
 
 static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
