@@ -23,7 +23,8 @@
 // trip through L2.  The other CTAs take the remaining tasks
 // in a fixed order from an atomic counter: S(., 0), then for each k the
 // solves S(i, k+1) (i >= k+3) and the updates U(., ., k), the update that
-// gates the next panel first.  Every task depends only on chain tasks and on
+// gates the next panel first; the last update of the chain's next solve
+// S(k+2, k+1) leads the list for panel k.  Every task depends only on chain tasks and on
 // tasks earlier in the list, so with all CTAs resident the lowest unfinished
 // task can always run.
 //
@@ -678,6 +679,14 @@ __device__ __forceinline__ void solve_by_inverse(const T* C, const T* X, T acc[1
 }
 
 template <typename T>
+__device__ __forceinline__ void smem_to_acc(const T* s, T acc[16]) {
+#pragma unroll
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) acc[TileMMA<T>::idx(rs, cs)] = s[acc_row(rs) * LDA + acc_col(cs)];
+}
+
+template <typename T>
 __device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
 #pragma unroll
   for (int rs = 0; rs < 2; ++rs)
@@ -692,23 +701,34 @@ template <typename T>
 constexpr int chain_smem_elems() { return 4 * NB * LDA + factor_smem_elems<T>(); }
 
 // The chain CTA: F(0), S(1, 0), F(1), S(2, 1), ... with L(k, k-1) and
-// inv(L_kk) kept in shared memory from one task to the next.
+// inv(L_kk) kept in shared memory from one task to the next.  The last
+// update of S(k+1, k) (with panel k-1) is a worker task that runs during
+// F(k); while S(k+1, k) runs, the next diagonal tile is prefetched into shared
+// memory if its updates by the workers are already complete.
 template <typename T>
 __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
+  __shared__ int s_pf;
   T* Cp = reinterpret_cast<T*>(smem);  // L(k, k-1), the previous solve's result
   T* Cn = Cp + NB * LDA;               // this step's solve input / result L(k+1, k)
   T* X = Cn + NB * LDA;                // inv(L_kk)
-  T* sA = X + NB * LDA;                // L_kk during F(k); then staged L(k+1, k-1)
+  T* sA = X + NB * LDA;                // prefetched A_kk; L_kk at the end of F(k)
   T* fs = sA + NB * LDA;               // factor scratch
   const int nt = a.nt;
+  bool pf = false;  // A_kk prefetched into sA
   for (int k = 0; k < nt; ++k) {
     T acc[16];
     // F(k): A_kk after updates 0 .. k-2 (other CTAs), minus L(k,k-1) L(k,k-1)^T
     TRACE(0, a.ntasks + 2 * k);
     TRACE(3, a.ntasks + 2 * k);
     if (k > 0) {
-      if (!wait_geq(a, a.upd + k * nt + k, k - 1, s_ok)) return;
-      load_acc(tile<T>(a, k, k), a.ld, acc);
+      if (pf) {
+        cp_async_wait_all();
+        __syncthreads();
+        smem_to_acc(sA, acc);
+      } else {
+        if (!wait_geq(a, a.upd + k * nt + k, k - 1, s_ok)) return;
+        load_acc(tile<T>(a, k, k), a.ld, acc);
+      }
       TileMMA<T>::sub(Cp, Cp, acc);  // Cp is complete: the last solve ended with a barrier
     } else {
       load_acc(tile<T>(a, 0, 0), a.ld, acc);
@@ -718,22 +738,19 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
     publish(a.fin + k * nt + k, 1);
     TRACE(2, a.ntasks + 2 * k);
     if (k + 1 == nt) return;
-    // S(k+1, k): A(k+1,k) after updates 0 .. k-2, minus L(k+1,k-1) L(k,k-1)^T,
-    // times inv(L_kk)^T
+    // S(k+1, k): A(k+1,k) after updates 0 .. k-1 (other CTAs), times inv(L_kk)^T
     TRACE(0, a.ntasks + 2 * k + 1);
     TRACE(3, a.ntasks + 2 * k + 1);
+    if (threadIdx.x == 0) s_pf = ld_acquire(a.upd + (k + 1) * nt + k + 1) >= k;
     if (k > 0) {
-      const int* fl[2] = {a.fin + (k + 1) * nt + k - 1, a.upd + (k + 1) * nt + k};
-      const int tg[2] = {1, k - 1};
-      if (!wait_all(a, fl, tg, 2, s_ok)) return;
-      stage_async(tile<T>(a, k + 1, k - 1), a.ld, sA, LDA);
-      load_acc(tile<T>(a, k + 1, k), a.ld, acc);
-      cp_async_wait_all();
-      __syncthreads();
-      TileMMA<T>::sub(sA, Cp, acc);
+      if (!wait_geq(a, a.upd + (k + 1) * nt + k, k, s_ok)) return;
     } else {
-      load_acc(tile<T>(a, 1, 0), a.ld, acc);
+      __syncthreads();
     }
+    // thread 0's acquire and the barrier order the prefetch after the updates
+    pf = s_pf != 0;
+    if (pf) stage_async(tile<T>(a, k + 1, k + 1), a.ld, sA, LDA);
+    load_acc(tile<T>(a, k + 1, k), a.ld, acc);
     TRACE(1, a.ntasks + 2 * k + 1);
     acc_to_smem(acc, Cn);
     __syncthreads();
@@ -823,9 +840,12 @@ int get_task_table(int nt, const int4** out, int* count) {
   std::vector<int4> t;
   for (int i = 2; i < nt; ++i) t.push_back(make_int4(TASK_S, i, 0, 0));
   for (int k = 0; k + 1 < nt; ++k) {
+    // the last update of the chain's S(k+2, k+1), first: it runs during F(k+1)
+    if (k + 2 < nt) t.push_back(make_int4(TASK_U, k + 2, k + 1, k));
     for (int i = k + 3; i < nt; ++i) t.push_back(make_int4(TASK_S, i, k + 1, k + 1));
-    // column k+1 of the update with panel k is fused into F(k+1) / S(., k+1);
-    // the plain updates cover columns >= k+2, the one gating the next panel first
+    // the rest of column k+1 of the update with panel k is fused into F(k+1)
+    // and the workers' S(., k+1); the plain updates cover columns >= k+2, the
+    // one gating the next panel first
     for (int jj = k + 2; jj < nt; ++jj)
       for (int i = jj; i < nt; ++i) t.push_back(make_int4(TASK_U, i, jj, k));
   }
