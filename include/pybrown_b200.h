@@ -231,6 +231,49 @@ PBG_API int pbg_run(pbg_system *sys, long long j0, int n_steps, double dt, int d
             int chol_freq, const double *pool, long long pool_len, void *stream);
 PBG_API int pbg_run_report(pbg_system *sys, pbg_step_report *out, void *stream);
 
+/* ---- Tier 3: batched replicas -------------------------------------------
+ * No counterpart in the reference, which advances one Box per process.  A
+ * batch holds many independent BD systems (rpy or rpy_smith hydrodynamics,
+ * Ermak scheme, one precision and Ewald parameter set for all) and advances
+ * them together; each replica follows Box.propagate (box.py:150-250) on its
+ * own positions, radii, box, temperature and noise.  Replicas can be added
+ * and removed between steps; slot ids stay valid until removal.  Arrays
+ * indexed by slot (mask, accepted, status) have pbg_batch_slots() entries.
+ * A step: pbg_batch_step_begin, then for the replicas still moving noise
+ * (pbg_batch_set_noise or pbg_batch_fill_noise) and pbg_batch_step_attempt
+ * until each is accepted (box.py:219-248), then pbg_batch_step_end. */
+typedef struct pbg_batch pbg_batch;
+
+/* precision, hydrodynamics, propagation_scheme and the Ewald fields of tmpl
+ * apply to every replica. */
+PBG_API int pbg_batch_create(const pbg_params *tmpl, pbg_batch **out);
+PBG_API int pbg_batch_destroy(pbg_batch *b);
+/* Device bytes one replica of n_beads takes (matrices, factor, tables, state). */
+PBG_API long long pbg_batch_footprint(int precision, int hydrodynamics, int ewald_imag, int n_beads);
+/* p: n_beads, box_length, kBT, viscosity, check_overlaps, overlap_treshold.
+ * pos (3N), radii (N): host or device memory. */
+PBG_API int pbg_batch_add(pbg_batch *b, const pbg_params *p, const double *pos, const double *radii, int *slot);
+PBG_API int pbg_batch_remove(pbg_batch *b, int slot);
+PBG_API int pbg_batch_slots(pbg_batch *b);
+PBG_API int pbg_batch_set_positions(pbg_batch *b, int slot, const double *pos);
+PBG_API int pbg_batch_get_positions(pbg_batch *b, int slot, double *out);
+/* External force (3N), or NULL for none. */
+PBG_API int pbg_batch_set_force(pbg_batch *b, int slot, const double *F);
+/* Noise of the next attempt (3N normals, host or device memory). */
+PBG_API int pbg_batch_set_noise(pbg_batch *b, int slot, const double *xi);
+/* Counter-based device noise (Philox-4x32-10 + Box-Muller): stream position
+ * `draws` of the stream `seed`; pbg_batch_fill_noise fills the masked
+ * replicas and advances each stream by 3N draws (rounded up to even). */
+PBG_API int pbg_batch_set_seed(pbg_batch *b, int slot, unsigned long long seed, unsigned long long draws);
+PBG_API int pbg_batch_get_draws(pbg_batch *b, int slot, unsigned long long *draws);
+PBG_API int pbg_batch_fill_noise(pbg_batch *b, const unsigned char *mask, void *stream);
+PBG_API int pbg_batch_step_begin(pbg_batch *b, double dt, int build_D, int cholesky, void *stream);
+PBG_API int pbg_batch_step_attempt(pbg_batch *b, const unsigned char *mask, unsigned char *accepted, void *stream);
+/* status[slot]: 0, the first non-positive pivot (1-based), or -1 (a wait gave up). */
+PBG_API int pbg_batch_step_end(pbg_batch *b, int *status, void *stream);
+/* D or B (PBG_MAT_D / PBG_MAT_B) of one replica, 3N x 3N FP64 row-major host array. */
+PBG_API int pbg_batch_get_matrix(pbg_batch *b, int slot, int which, double *out);
+
 #ifdef __cplusplus
 }
 #endif

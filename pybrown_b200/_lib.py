@@ -104,6 +104,23 @@ _SIGNATURES = {
     "pbg_step_end": (_i, [_vp, _vp]),
     "pbg_run": (_i, [_vp, _ll, _i, _d, _i, _i, _i, _vp, _ll, _vp]),
     "pbg_run_report": (_i, [_vp, ctypes.POINTER(PbgStepReport), _vp]),
+    "pbg_batch_create": (_i, [ctypes.POINTER(PbgParams), ctypes.POINTER(_vp)]),
+    "pbg_batch_destroy": (_i, [_vp]),
+    "pbg_batch_footprint": (_ll, [_i, _i, _i, _i]),
+    "pbg_batch_add": (_i, [_vp, ctypes.POINTER(PbgParams), _vp, _vp, _ip]),
+    "pbg_batch_remove": (_i, [_vp, _i]),
+    "pbg_batch_slots": (_i, [_vp]),
+    "pbg_batch_set_positions": (_i, [_vp, _i, _vp]),
+    "pbg_batch_get_positions": (_i, [_vp, _i, _vp]),
+    "pbg_batch_set_force": (_i, [_vp, _i, _vp]),
+    "pbg_batch_set_noise": (_i, [_vp, _i, _vp]),
+    "pbg_batch_set_seed": (_i, [_vp, _i, ctypes.c_ulonglong, ctypes.c_ulonglong]),
+    "pbg_batch_get_draws": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "pbg_batch_fill_noise": (_i, [_vp, _vp, _vp]),
+    "pbg_batch_step_begin": (_i, [_vp, _d, _i, _i, _vp]),
+    "pbg_batch_step_attempt": (_i, [_vp, _vp, _vp, _vp]),
+    "pbg_batch_step_end": (_i, [_vp, _vp, _vp]),
+    "pbg_batch_get_matrix": (_i, [_vp, _i, _i, _vp]),
 }
 
 

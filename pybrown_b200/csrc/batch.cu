@@ -1,0 +1,728 @@
+// Batched replicas: many independent BD systems with hydrodynamic
+// interactions (rpy / rpy_smith, Ermak-McCammon scheme) advanced together.
+//
+// Every replica follows Box.propagate (src/bdsim/pyBrown/box.py:150-250) on
+// its own positions, radii, box and noise stream, exactly as a single system
+// would: D from the RPY (or Smith-Ewald RPY) tensor, B = chol(D), the
+// deterministic step (dt/kBT) D F, then attempts of the stochastic step
+// sqrt(2 dt) B xi that are undone on a bead overlap and redrawn.
+//
+// Each replica owns its device buffers (allocated when it is added).  The
+// per-replica descriptors and work lists that the kernels read are rebuilt
+// only when the membership changes, so replicas can join and leave between
+// steps while the others keep their state on the device.  One step is a
+// fixed sequence of launches over all replicas: phase tables and Ewald tiles
+// (one work list), the padded copy into B, one cooperative data-flow Cholesky
+// over every replica's tiles, then the per-replica vector kernels (replica =
+// blockIdx.y).  Replicas never interact, and each one's arithmetic does not
+// depend on which other replicas share the batch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pybrown_b200.h"
+
+namespace pbg {
+
+struct BatchReplica {
+  pbg_params p;
+  int N = 0, n = 0, ld = 0, nt = 0;
+  double scale = 0;  // kBT 1e19 / eta: D = scale * M (box.py:498)
+  double *pos = nullptr, *radii = nullptr, *force = nullptr, *U = nullptr, *xi = nullptr;
+  void *D = nullptr, *B = nullptr, *invdiag = nullptr, *phase = nullptr;
+  bool has_force = false;
+  unsigned long long seed = 0, draws = 0;
+};
+
+// What the vector kernels need of one replica.
+struct BatchDev {
+  double* pos;
+  const double* radii;
+  const double* force;
+  double* U;
+  double* xi;
+  const void* D;
+  void* B;
+  double L, thr, kBT;
+  int N, n, ld, check, has_force, pad;
+};
+
+}  // namespace pbg
+
+struct pbg_batch {
+  int precision = PBG_PREC_MIXED;
+  int hydrodynamics = PBG_HI_RPY_SMITH;
+  double alpha = 0;
+  int m_max = 0, n_max = 0;
+  const pbg::EwaldTables* tables = nullptr;
+  std::vector<pbg::BatchReplica*> slots;
+  // active replicas (slot ids) in the order of the device arrays
+  std::vector<int> active;
+  bool dirty = true;
+  double dt = 0;
+  bool in_step = false;
+  // device arrays of the current membership
+  pbg::BatchDev* d_reps = nullptr;
+  void* d_rpy = nullptr;
+  int4* d_ework = nullptr;
+  int n_ework = 0;
+  pbg::CholRep* d_chol = nullptr;
+  int4* d_tasks = nullptr;
+  int ntasks = 0;
+  int* d_flags = nullptr;  // [4 ctl][per replica: upd nt^2, fin nt^2][R infos]
+  size_t flag_ints = 0;
+  int* d_info = nullptr;
+  int* d_ovl = nullptr;
+  unsigned char* d_mask = nullptr;
+  unsigned long long* d_stream = nullptr;  // [R][2]: seed, draws of each noise stream
+  int* h_ovl = nullptr;  // pinned, read after a stream synchronisation
+  int* h_info = nullptr;
+  std::vector<unsigned char> mask;  // of the last upload, active order
+  size_t cap = 0;  // capacity of the per-replica device/pinned arrays
+  int max_n = 0;
+};
+
+namespace pbg {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double s) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// B = lower(D) with the identity beyond n and zeros above the diagonal.
+template <typename T>
+__global__ void batch_copy_lower_kernel(const BatchDev* __restrict__ reps) {
+  const BatchDev& r = reps[blockIdx.y];
+  const T* src = static_cast<const T*>(r.D);
+  T* dst = static_cast<T*>(r.B);
+  const int n = r.n, ld = r.ld;
+  const long long total = (long long)ld * ld;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(t / ld), col = (int)(t % ld);
+    T v;
+    if (row < n && col < n) v = col <= row ? src[t] : (T)0;
+    else v = (T)(row == col ? 1 : 0);
+    dst[t] = v;
+  }
+}
+
+// Deterministic step (box.py:353-362) for replicas with a force:
+// pos += ((dt/kBT) D @ F * 1) * 1, one warp per row.
+template <typename T>
+__global__ void batch_det_kernel(const BatchDev* __restrict__ reps, double dt) {
+  const BatchDev& r = reps[blockIdx.y];
+  if (!r.has_force) return;
+  const T* D = static_cast<const T*>(r.D);
+  const double c = dt / r.kBT;
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < r.n; row += gridDim.x * warps) {
+    const T* a = D + (size_t)row * r.ld;
+    double s = 0.0;
+    for (int j = lane; j < r.n; j += 32) s += (c * (double)a[j]) * r.force[j];
+    s = warp_sum(s);
+    // the displacement waits in U until every row is done (see batch_det_move)
+    if (lane == 0) r.U[row] = (s * 1.0) * 1.0;
+  }
+}
+
+__global__ void batch_det_move_kernel(const BatchDev* __restrict__ reps) {
+  const BatchDev& r = reps[blockIdx.y];
+  if (!r.has_force) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) r.pos[i] += r.U[i];
+}
+
+// U = B xi for the masked replicas (box.py:371; B lower triangular).
+template <typename T>
+__global__ void batch_trmv_kernel(const BatchDev* __restrict__ reps, const unsigned char* __restrict__ mask) {
+  if (!mask[blockIdx.y]) return;
+  const BatchDev& r = reps[blockIdx.y];
+  const T* B = static_cast<const T*>(r.B);
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < r.n; row += gridDim.x * warps) {
+    const T* b = B + (size_t)row * r.ld;
+    double s = 0.0;
+    for (int j = lane; j <= row; j += 32) s += (double)b[j] * r.xi[j];
+    s = warp_sum(s);
+    if (lane == 0) r.U[row] = s;
+  }
+}
+
+// Stochastic step (box.py:366-375): pos += (U sqrt(2 dt)) * mult, for the
+// masked replicas; with `undo`, only those whose overlap flag is set.
+__global__ void batch_move_kernel(const BatchDev* __restrict__ reps, const unsigned char* __restrict__ mask,
+                                  const int* __restrict__ ovl, double s1, double mult, int undo) {
+  if (!mask[blockIdx.y]) return;
+  if (undo && !ovl[blockIdx.y]) return;
+  const BatchDev& r = reps[blockIdx.y];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x)
+    r.pos[i] += (r.U[i] * s1) * mult;
+}
+
+// Overlap test of the masked replicas (bead.c:169-218), no bonded pairs.
+__global__ void batch_overlap_kernel(const BatchDev* __restrict__ reps, const unsigned char* __restrict__ mask,
+                                     int* __restrict__ ovl) {
+  if (!mask[blockIdx.y]) return;
+  const BatchDev& r = reps[blockIdx.y];
+  if (!r.check) return;
+  const long long npairs = (long long)r.N * (r.N - 1) / 2;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npairs;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (ovl[blockIdx.y]) return;
+    int i, j;
+    pair_from_linear(p, i, j);
+    if (pair_overlaps(r.pos, r.radii, i, j, r.L, r.thr)) {
+      atomicOr(ovl + blockIdx.y, 1);
+      return;
+    }
+  }
+}
+
+__global__ void batch_wrap_kernel(const BatchDev* __restrict__ reps) {
+  const BatchDev& r = reps[blockIdx.y];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x)
+    r.pos[i] = pbg_wrap(r.pos[i], r.L);
+}
+
+// Counter-based normal variates for a replica's noise stream: Philox-4x32-10
+// (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC 2011) keyed by the replica's seed, counter = pair index of the draw,
+// and the Box-Muller transform of two 53-bit uniforms.  Draw d of a stream
+// depends only on (seed, d), never on the other replicas of the batch.
+__device__ __forceinline__ void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t m0 = 0xD2511F53u, m1 = 0xCD9E8D57u;
+  const uint32_t hi0 = __umulhi(m0, c[0]), lo0 = m0 * c[0];
+  const uint32_t hi1 = __umulhi(m1, c[2]), lo1 = m1 * c[2];
+  const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+  c[0] = n0;
+  c[1] = lo1;
+  c[2] = n2;
+  c[3] = lo0;
+}
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    philox_round(c, k0, k1);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+__device__ __forceinline__ double u53(uint32_t hi, uint32_t lo) {
+  const unsigned long long v = ((unsigned long long)hi << 32 | lo) >> 11;
+  return ((double)v + 0.5) * (1.0 / 9007199254740992.0);  // (0, 1)
+}
+
+__global__ void batch_noise_kernel(const BatchDev* __restrict__ reps, const unsigned char* __restrict__ mask,
+                                   const unsigned long long* __restrict__ streams) {
+  if (!mask[blockIdx.y]) return;
+  const BatchDev& r = reps[blockIdx.y];
+  const unsigned long long seed = streams[2 * blockIdx.y], base = streams[2 * blockIdx.y + 1] / 2;  // even
+  const int pairs = (r.n + 1) / 2;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pairs; q += gridDim.x * blockDim.x) {
+    const unsigned long long ctr = base + (unsigned long long)q;
+    uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double u1 = u53(c[0], c[1]), u2 = u53(c[2], c[3]);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    r.xi[2 * q] = rad * cs;
+    if (2 * q + 1 < r.n) r.xi[2 * q + 1] = rad * sn;
+  }
+}
+
+inline size_t elem_size(int precision) { return precision == PBG_PREC_FP64 ? 8 : 4; }
+
+void free_replica(BatchReplica* r) {
+  if (!r) return;
+  void* bufs[] = {r->pos, r->radii, r->force, r->U, r->xi, r->D, r->B, r->invdiag, r->phase};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  delete r;
+}
+
+template <typename P>
+void free_dev(P*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Rebuilds the device descriptors and work lists of the current membership.
+int rebuild(pbg_batch* b) {
+  b->active.clear();
+  for (int s = 0; s < (int)b->slots.size(); ++s)
+    if (b->slots[s]) b->active.push_back(s);
+  const int R = (int)b->active.size();
+  free_dev(b->d_reps);
+  free_dev(b->d_rpy);
+  free_dev(b->d_ework);
+  free_dev(b->d_chol);
+  free_dev(b->d_tasks);
+  free_dev(b->d_flags);
+  b->n_ework = b->ntasks = 0;
+  if ((size_t)R > b->cap || !b->d_ovl) {
+    free_dev(b->d_ovl);
+    free_dev(b->d_mask);
+    free_dev(b->d_stream);
+    if (b->h_ovl) cudaFreeHost(b->h_ovl);
+    if (b->h_info) cudaFreeHost(b->h_info);
+    b->h_ovl = b->h_info = nullptr;
+    b->cap = std::max<size_t>(R, 16);
+    PBG_CUDA_TRY(cudaMalloc(&b->d_ovl, b->cap * sizeof(int)));
+    PBG_CUDA_TRY(cudaMalloc(&b->d_mask, b->cap));
+    PBG_CUDA_TRY(cudaMalloc(&b->d_stream, 2 * b->cap * sizeof(unsigned long long)));
+    PBG_CUDA_TRY(cudaMallocHost(&b->h_ovl, b->cap * sizeof(int)));
+    PBG_CUDA_TRY(cudaMallocHost(&b->h_info, b->cap * sizeof(int)));
+  }
+  b->max_n = 0;
+  if (R == 0) {
+    b->dirty = false;
+    return PBG_OK;
+  }
+  std::vector<BatchDev> reps(R);
+  std::vector<unsigned char> rpy(R * rpy_batch_arg_bytes());
+  std::vector<int4> ework;
+  std::vector<int> nts(R);
+  size_t flag_ints = 4;
+  std::vector<size_t> flag_off(R);
+  for (int q = 0; q < R; ++q) {
+    const BatchReplica* r = b->slots[b->active[q]];
+    flag_off[q] = flag_ints;
+    flag_ints += 2 * (size_t)r->nt * r->nt;
+    nts[q] = r->nt;
+    b->max_n = std::max(b->max_n, r->n);
+  }
+  const size_t info_off = flag_ints;
+  flag_ints += R;
+  b->flag_ints = flag_ints;
+  PBG_CUDA_TRY(cudaMalloc(&b->d_flags, flag_ints * sizeof(int)));
+  b->d_info = b->d_flags + info_off;
+  std::vector<CholRep> chol(R);
+  const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
+  for (int q = 0; q < R; ++q) {
+    BatchReplica* r = b->slots[b->active[q]];
+    BatchDev& d = reps[q];
+    d.pos = r->pos;
+    d.radii = r->radii;
+    d.force = r->force;
+    d.U = r->U;
+    d.xi = r->xi;
+    d.D = r->D;
+    d.B = r->B;
+    d.L = r->p.box_length;
+    d.thr = r->p.overlap_treshold;
+    d.kBT = r->p.kBT;
+    d.N = r->N;
+    d.n = r->n;
+    d.ld = r->ld;
+    d.check = r->p.check_overlaps;
+    d.has_force = r->has_force;
+    d.pad = 0;
+    rpy_batch_arg(r->pos, r->radii, r->N, r->p.box_length, smith, b->tables, r->scale, r->D, r->ld, r->phase,
+                  rpy.data() + q * rpy_batch_arg_bytes());
+    rpy_batch_work(q, r->N, ework);
+    CholRep& c = chol[q];
+    c.A = r->B;
+    c.invdiag = r->invdiag;
+    c.upd = b->d_flags + flag_off[q];
+    c.fin = c.upd + (size_t)r->nt * r->nt;
+    c.info = b->d_info + q;
+    c.ld = r->ld;
+    c.n = r->n;
+    c.nt = r->nt;
+    c.pad = 0;
+  }
+  std::vector<int4> tasks;
+  cholesky_batch_tasks(nts, tasks);
+  PBG_CUDA_TRY(cudaMalloc(&b->d_reps, R * sizeof(BatchDev)));
+  PBG_CUDA_TRY(cudaMalloc(&b->d_rpy, rpy.size()));
+  PBG_CUDA_TRY(cudaMalloc(&b->d_ework, ework.size() * sizeof(int4)));
+  PBG_CUDA_TRY(cudaMalloc(&b->d_chol, R * sizeof(CholRep)));
+  PBG_CUDA_TRY(cudaMalloc(&b->d_tasks, std::max<size_t>(tasks.size(), 1) * sizeof(int4)));
+  PBG_CUDA_TRY(cudaMemcpy(b->d_reps, reps.data(), R * sizeof(BatchDev), cudaMemcpyHostToDevice));
+  PBG_CUDA_TRY(cudaMemcpy(b->d_rpy, rpy.data(), rpy.size(), cudaMemcpyHostToDevice));
+  PBG_CUDA_TRY(cudaMemcpy(b->d_ework, ework.data(), ework.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  PBG_CUDA_TRY(cudaMemcpy(b->d_chol, chol.data(), R * sizeof(CholRep), cudaMemcpyHostToDevice));
+  if (!tasks.empty())
+    PBG_CUDA_TRY(cudaMemcpy(b->d_tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  b->n_ework = (int)ework.size();
+  b->ntasks = (int)tasks.size();
+  b->dirty = false;
+  return PBG_OK;
+}
+
+inline dim3 rows_grid(const pbg_batch* b, int per_block) {
+  const int x = std::max(1, std::min(64, (b->max_n + per_block - 1) / per_block));
+  return dim3(x, (unsigned)b->active.size());
+}
+
+// Copies the host mask (indexed by slot, or all when null) to the device in
+// the order of the active replicas.  Returns the number of masked replicas.
+// Small uploads go from pageable memory: the copy is staged before the call
+// returns, so the host vectors can change right away.
+int upload_mask(pbg_batch* b, const unsigned char* mask, cudaStream_t st, int* count) {
+  const int R = (int)b->active.size();
+  b->mask.assign(R, 0);
+  int c = 0;
+  for (int q = 0; q < R; ++q) {
+    b->mask[q] = mask ? (mask[b->active[q]] ? 1 : 0) : 1;
+    c += b->mask[q];
+  }
+  *count = c;
+  if (R) PBG_CUDA_TRY(cudaMemcpyAsync(b->d_mask, b->mask.data(), R, cudaMemcpyHostToDevice, st));
+  return PBG_OK;
+}
+
+}  // namespace
+}  // namespace pbg
+
+using namespace pbg;
+
+extern "C" {
+
+PBG_API int pbg_batch_create(const pbg_params* tmpl, pbg_batch** out) {
+  if (!tmpl || !out) return PBG_ERR_ARG;
+  if (tmpl->hydrodynamics != PBG_HI_RPY && tmpl->hydrodynamics != PBG_HI_RPY_SMITH) {
+    pbg_set_error_message("batched replicas support the rpy and rpy_smith hydrodynamics");
+    return PBG_ERR_ARG;
+  }
+  if (tmpl->precision != PBG_PREC_FP64 && tmpl->precision != PBG_PREC_MIXED) return PBG_ERR_ARG;
+  if (tmpl->propagation_scheme != PBG_SCHEME_ERMAK) {
+    pbg_set_error_message("batched replicas support the ermak propagation scheme");
+    return PBG_ERR_ARG;
+  }
+  auto* b = new pbg_batch();
+  b->precision = tmpl->precision;
+  b->hydrodynamics = tmpl->hydrodynamics;
+  if (b->hydrodynamics == PBG_HI_RPY_SMITH) {
+    b->alpha = tmpl->ewald_alpha;
+    b->m_max = tmpl->ewald_real;
+    b->n_max = tmpl->ewald_imag;
+    int rc = get_ewald_tables(b->alpha, b->m_max, b->n_max, &b->tables);
+    if (rc) {
+      delete b;
+      return rc;
+    }
+  }
+  *out = b;
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_destroy(pbg_batch* b) {
+  if (!b) return PBG_OK;
+  cudaDeviceSynchronize();
+  for (auto* r : b->slots) free_replica(r);
+  free_dev(b->d_reps);
+  free_dev(b->d_rpy);
+  free_dev(b->d_ework);
+  free_dev(b->d_chol);
+  free_dev(b->d_tasks);
+  free_dev(b->d_flags);
+  free_dev(b->d_ovl);
+  free_dev(b->d_mask);
+  free_dev(b->d_stream);
+  if (b->h_ovl) cudaFreeHost(b->h_ovl);
+  if (b->h_info) cudaFreeHost(b->h_info);
+  delete b;
+  return PBG_OK;
+}
+
+// Device bytes a replica of n_beads takes in a batch of this precision.
+PBG_API long long pbg_batch_footprint(int precision, int hydrodynamics, int ewald_imag, int n_beads) {
+  const long long n = 3LL * n_beads, ld = (n + PBG_TILE - 1) / PBG_TILE * PBG_TILE, nt = ld / PBG_TILE;
+  const long long es = elem_size(precision);
+  long long n_recip = 0;
+  if (hydrodynamics == PBG_HI_RPY_SMITH)
+    for (int x = -ewald_imag; x <= ewald_imag; ++x)
+      for (int y = -ewald_imag; y <= ewald_imag; ++y)
+        for (int z = -ewald_imag; z <= ewald_imag; ++z)
+          if (std::abs(x) + std::abs(y) + std::abs(z) <= ewald_imag && (x || y || z)) ++n_recip;
+  n_recip /= 2;
+  return 2 * ld * ld * es + nt * PBG_TILE * PBG_TILE * es + (long long)n_beads * n_recip * 2 * es +
+         (4 * ld + 4 * n_beads) * 8 + 2 * nt * nt * 4;
+}
+
+PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, const double* radii, int* slot) {
+  if (!b || !p || !pos || !radii || !slot || p->n_beads <= 0 || !(p->box_length > 0) || !(p->kBT > 0) ||
+      !(p->viscosity > 0))
+    return PBG_ERR_ARG;
+  if (b->in_step) {
+    pbg_set_error_message("pbg_batch_add inside a step");
+    return PBG_ERR_STATE;
+  }
+  auto* r = new BatchReplica();
+  r->p = *p;
+  r->N = p->n_beads;
+  r->n = 3 * r->N;
+  r->ld = (r->n + PBG_TILE - 1) / PBG_TILE * PBG_TILE;
+  r->nt = r->ld / PBG_TILE;
+  r->scale = p->kBT * 1e19 / p->viscosity;
+  const size_t es = elem_size(b->precision), ld = r->ld;
+  bool ok = cudaMalloc(&r->pos, r->n * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&r->radii, r->N * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&r->force, ld * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&r->U, ld * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&r->xi, ld * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&r->D, ld * ld * es) == cudaSuccess && cudaMalloc(&r->B, ld * ld * es) == cudaSuccess &&
+            cudaMalloc(&r->invdiag, (size_t)r->nt * PBG_TILE * PBG_TILE * es) == cudaSuccess;
+  const size_t ph = phase_scratch_bytes(r->N, b->tables, b->precision);
+  if (ok && ph) ok = cudaMalloc(&r->phase, ph) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    free_replica(r);
+    pbg_set_error_message("out of device memory adding a replica of %d beads", p->n_beads);
+    return PBG_ERR_NOMEM;
+  }
+  cudaMemset(r->force, 0, ld * sizeof(double));
+  cudaMemset(r->U, 0, ld * sizeof(double));
+  cudaMemset(r->xi, 0, ld * sizeof(double));
+  PBG_CUDA_TRY(cudaMemcpy(r->pos, pos, r->n * sizeof(double), cudaMemcpyDefault));
+  PBG_CUDA_TRY(cudaMemcpy(r->radii, radii, r->N * sizeof(double), cudaMemcpyDefault));
+  int s = 0;
+  while (s < (int)b->slots.size() && b->slots[s]) ++s;
+  if (s == (int)b->slots.size()) b->slots.push_back(nullptr);
+  b->slots[s] = r;
+  b->dirty = true;
+  *slot = s;
+  return PBG_OK;
+}
+
+static BatchReplica* slot_of(pbg_batch* b, int slot) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size()) return nullptr;
+  return b->slots[slot];
+}
+
+PBG_API int pbg_batch_remove(pbg_batch* b, int slot) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r) return PBG_ERR_ARG;
+  if (b->in_step) {
+    pbg_set_error_message("pbg_batch_remove inside a step");
+    return PBG_ERR_STATE;
+  }
+  PBG_CUDA_TRY(cudaDeviceSynchronize());
+  free_replica(r);
+  b->slots[slot] = nullptr;
+  b->dirty = true;
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_slots(pbg_batch* b) { return b ? (int)b->slots.size() : 0; }
+
+PBG_API int pbg_batch_set_positions(pbg_batch* b, int slot, const double* pos) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !pos) return PBG_ERR_ARG;
+  PBG_CUDA_TRY(cudaMemcpy(r->pos, pos, r->n * sizeof(double), cudaMemcpyDefault));
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_get_positions(pbg_batch* b, int slot, double* out) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !out) return PBG_ERR_ARG;
+  PBG_CUDA_TRY(cudaMemcpy(out, r->pos, r->n * sizeof(double), cudaMemcpyDefault));
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_set_force(pbg_batch* b, int slot, const double* F) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r) return PBG_ERR_ARG;
+  if (F) PBG_CUDA_TRY(cudaMemcpy(r->force, F, r->n * sizeof(double), cudaMemcpyDefault));
+  else PBG_CUDA_TRY(cudaMemset(r->force, 0, r->n * sizeof(double)));
+  if (r->has_force != (F != nullptr)) b->dirty = true;
+  r->has_force = F != nullptr;
+  return PBG_OK;
+}
+
+// Noise for the next attempt of one replica (3N normals, host or device memory).
+PBG_API int pbg_batch_set_noise(pbg_batch* b, int slot, const double* xi) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !xi) return PBG_ERR_ARG;
+  PBG_CUDA_TRY(cudaMemcpy(r->xi, xi, r->n * sizeof(double), cudaMemcpyDefault));
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_set_seed(pbg_batch* b, int slot, unsigned long long seed, unsigned long long draws) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r) return PBG_ERR_ARG;
+  r->seed = seed;
+  r->draws = draws + (draws & 1);
+  return PBG_OK;
+}
+
+PBG_API int pbg_batch_get_draws(pbg_batch* b, int slot, unsigned long long* draws) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !draws) return PBG_ERR_ARG;
+  *draws = r->draws;
+  return PBG_OK;
+}
+
+// Fills the masked replicas' noise from their counter-based streams and
+// advances each stream by 3N draws (rounded up to even).
+PBG_API int pbg_batch_fill_noise(pbg_batch* b, const unsigned char* mask, void* stream) {
+  if (!b) return PBG_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (b->dirty && (rc = rebuild(b))) return rc;
+  const int R = (int)b->active.size();
+  if (!R) return PBG_OK;
+  int count = 0;
+  if ((rc = upload_mask(b, mask, st, &count))) return rc;
+  if (!count) return PBG_OK;
+  // the stream positions of this fill (pageable staging, see upload_mask)
+  std::vector<unsigned long long> streams(2 * R);
+  for (int q = 0; q < R; ++q) {
+    const BatchReplica* r = b->slots[b->active[q]];
+    streams[2 * q] = r->seed;
+    streams[2 * q + 1] = r->draws;
+  }
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_stream, streams.data(), streams.size() * sizeof(unsigned long long),
+                               cudaMemcpyHostToDevice, st));
+  batch_noise_kernel<<<rows_grid(b, 512), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_stream);
+  PBG_CHECK_LAUNCH();
+  for (int q = 0; q < R; ++q)
+    if (b->mask[q]) {
+      BatchReplica* r = b->slots[b->active[q]];
+      r->draws += (unsigned long long)(r->n + (r->n & 1));
+    }
+  return PBG_OK;
+}
+
+// Builds D (build_D) and B = chol(D) (cholesky) of every replica and applies
+// the deterministic step of the replicas with a force.
+PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int cholesky, void* stream) {
+  if (!b || !(dt > 0)) return PBG_ERR_ARG;
+  if (b->in_step) {
+    pbg_set_error_message("pbg_batch_step_begin inside a step");
+    return PBG_ERR_STATE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (b->dirty && (rc = rebuild(b))) return rc;
+  b->dt = dt;
+  const int R = (int)b->active.size();
+  if (!R) {
+    b->in_step = true;
+    return PBG_OK;
+  }
+  const bool f64 = b->precision == PBG_PREC_FP64;
+  const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
+  if (build_D && (rc = launch_rpy_batch(b->precision, smith, b->tables, b->d_rpy, b->d_ework, b->n_ework, R, st)))
+    return rc;
+  if (cholesky) {
+    const dim3 g(64, R);
+    if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
+    else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+    PBG_CHECK_LAUNCH();
+    PBG_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st));
+    if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, st))) return rc;
+  }
+  bool any_force = false;
+  for (int s : b->active) any_force = any_force || b->slots[s]->has_force;
+  if (any_force) {
+    if (f64) batch_det_kernel<double><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
+    else batch_det_kernel<float><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
+    PBG_CHECK_LAUNCH();
+    batch_det_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps);
+    PBG_CHECK_LAUNCH();
+  }
+  b->in_step = true;
+  return PBG_OK;
+}
+
+// One stochastic attempt for the masked replicas (host array indexed by slot,
+// or null for all) with the noise already in place: U = B xi,
+// pos += U sqrt(2 dt), overlap test, undo on overlap.  accepted[slot] (host,
+// optional) is set to 1 or 0 for the masked replicas.
+PBG_API int pbg_batch_step_attempt(pbg_batch* b, const unsigned char* mask, unsigned char* accepted, void* stream) {
+  if (!b) return PBG_ERR_ARG;
+  if (!b->in_step) {
+    pbg_set_error_message("pbg_batch_step_attempt outside a step");
+    return PBG_ERR_STATE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int R = (int)b->active.size();
+  if (!R) return PBG_OK;
+  int count = 0, rc;
+  if ((rc = upload_mask(b, mask, st, &count))) return rc;
+  if (!count) return PBG_OK;
+  const bool f64 = b->precision == PBG_PREC_FP64;
+  const double s1 = std::sqrt(2 * b->dt);
+  if (f64) batch_trmv_kernel<double><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, b->d_mask);
+  else batch_trmv_kernel<float><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, b->d_mask);
+  PBG_CHECK_LAUNCH();
+  batch_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl, s1, 1.0, 0);
+  PBG_CHECK_LAUNCH();
+  PBG_CUDA_TRY(cudaMemsetAsync(b->d_ovl, 0, R * sizeof(int), st));
+  batch_overlap_kernel<<<dim3(64, R), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl);
+  PBG_CHECK_LAUNCH();
+  batch_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl, s1, -1.0, 1);
+  PBG_CHECK_LAUNCH();
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->h_ovl, b->d_ovl, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (accepted)
+    for (int q = 0; q < R; ++q)
+      if (b->mask[q]) accepted[b->active[q]] = b->h_ovl[q] ? 0 : 1;
+  return PBG_OK;
+}
+
+// Wraps every replica into its box and reports the factorisation status of
+// the step: status[slot] (host, optional) = 0, or the first non-positive
+// pivot (1-based), or -1 when a wait of the factorisation gave up.
+PBG_API int pbg_batch_step_end(pbg_batch* b, int* status, void* stream) {
+  if (!b) return PBG_ERR_ARG;
+  if (!b->in_step) {
+    pbg_set_error_message("pbg_batch_step_end outside a step");
+    return PBG_ERR_STATE;
+  }
+  b->in_step = false;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int R = (int)b->active.size();
+  if (!R) return PBG_OK;
+  batch_wrap_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps);
+  PBG_CHECK_LAUNCH();
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->h_info, b->d_info, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  int worst = 0;
+  for (int q = 0; q < R; ++q) {
+    if (status) status[b->active[q]] = b->h_info[q];
+    if (b->h_info[q] < 0) worst = -1;
+    else if (b->h_info[q] > 0 && worst == 0) worst = 1;
+  }
+  if (worst < 0) {
+    pbg_set_error_message("a device-wide wait in the batched factorisation gave up");
+    return PBG_ERR_BARRIER;
+  }
+  if (worst > 0) {
+    pbg_set_error_message("a replica's diffusion matrix is not positive definite");
+    return PBG_ERR_NOT_SPD;
+  }
+  return PBG_OK;
+}
+
+// D or B (which = PBG_MAT_D / PBG_MAT_B) of one replica as a 3N x 3N FP64
+// row-major host array.
+PBG_API int pbg_batch_get_matrix(pbg_batch* b, int slot, int which, double* out) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !out || (which != PBG_MAT_D && which != PBG_MAT_B)) return PBG_ERR_ARG;
+  const size_t es = elem_size(b->precision), ld = r->ld;
+  std::vector<unsigned char> h(ld * ld * es);
+  PBG_CUDA_TRY(cudaMemcpy(h.data(), which == PBG_MAT_D ? r->D : r->B, h.size(), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < r->n; ++i)
+    for (int j = 0; j < r->n; ++j) {
+      double v;
+      if (es == 8) v = reinterpret_cast<const double*>(h.data())[(size_t)i * ld + j];
+      else v = reinterpret_cast<const float*>(h.data())[(size_t)i * ld + j];
+      if (which == PBG_MAT_B && j > i) v = 0.0;
+      out[(size_t)i * r->n + j] = v;
+    }
+  return PBG_OK;
+}
+
+}  // extern "C"

@@ -33,6 +33,7 @@
 // iteration count; on expiry the kernel raises an abort flag, marks info = -1
 // and every CTA returns.  Tile data written by other CTAs is read with
 // L2-coherent loads (ld.global.cg, cp.async.cg).
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -824,6 +825,79 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   }
 }
 
+// Batched factorisation: every task comes from the shared list (there is no
+// chain CTA); F(k) applies its last update itself.  Shared memory: two tiles
+// (sA / L_kk, sB / inv(L_kk)) and the factor scratch.
+template <typename T>
+constexpr int batch_smem_elems() { return 2 * NB * LDA + factor_smem_elems<T>(); }
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS, 1) chol_batch_kernel(const CholRep* __restrict__ reps,
+                                                                 const int4* __restrict__ tasks, int ntasks,
+                                                                 int* ctl) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_task, s_ok;
+  T* sA = reinterpret_cast<T*>(smem);
+  T* sB = sA + NB * LDA;
+  T* fs = sB + NB * LDA;
+  while (true) {
+    if (threadIdx.x == 0) s_task = ld_acquire(ctl + 1) ? ntasks : atomicAdd(ctl, 1);
+    __syncthreads();
+    const int t = s_task;
+    __syncthreads();
+    if (t >= ntasks) return;
+    const int4 tk = tasks[t];
+    const int type = tk.x & 3, i = tk.y, j = tk.z, k = tk.w;
+    const CholRep& R = reps[tk.x >> 2];
+    DFArgs a;
+    a.A = R.A;
+    a.ld = R.ld;
+    a.n = R.n;
+    a.nt = R.nt;
+    a.ntasks = ntasks;
+    a.tasks = tasks;
+    a.ctl = ctl;
+    a.upd = R.upd;
+    a.fin = R.fin;
+    a.info = R.info;
+    a.invdiag = R.invdiag;
+    a.err = reinterpret_cast<unsigned*>(ctl + 3);
+    const int nt = a.nt;
+    T acc[16];
+    if (type == TASK_U) {
+      const int* fl[3] = {a.fin + i * nt + k, a.fin + j * nt + k, a.upd + i * nt + j};
+      const int tg[3] = {1, 1, k};
+      if (!wait_all(a, fl, tg, 3, &s_ok)) return;
+      load_and_update(a, i, j, k, acc, sA, sB);
+      store_acc(tile<T>(a, i, j), a.ld, acc);
+      publish(a.upd + i * nt + j, k + 1);
+    } else {
+      const int col = j;
+      if (col > 0) {
+        const int* fl[3] = {a.fin + i * nt + col - 1, a.fin + col * nt + col - 1, a.upd + i * nt + col};
+        const int tg[3] = {1, 1, col - 1};
+        if (!wait_all(a, fl, tg, 3, &s_ok)) return;
+        load_and_update(a, i, col, col - 1, acc, sA, sB);  // ends with a barrier: smem is free
+      } else {
+        load_acc(tile<T>(a, i, col), a.ld, acc);
+      }
+      if (type == TASK_F) {
+        factor_tile<T>(a, col, acc, fs, sA, sB);
+      } else {
+        if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
+        stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);
+        acc_to_smem(acc, sA);
+        cp_async_wait_all();
+        __syncthreads();
+        solve_by_inverse(sA, sB, acc);
+        store_acc(tile<T>(a, i, col), a.ld, acc);
+      }
+      publish(a.fin + i * nt + col, 1);
+    }
+    __syncthreads();
+  }
+}
+
 std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
@@ -953,6 +1027,82 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
   unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 2 * (size_t)nt * nt);
   return precision == PBG_PREC_FP64 ? launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st)
                                     : launch_df<float>((float*)A, n, ld, info, invdiag, ints, err, st);
+}
+
+
+// Per replica: F(0), S(i, 0); then for each k: F(k+1), S(i, k+1) (i >= k+2),
+// U(i, j, k) (j >= k+2).  F(k+1) and S(., k+1) apply their update with panel
+// k themselves.  The replicas' lists are interleaved block by block, larger
+// matrices first within a block; each replica's own order is kept, so every
+// task depends only on earlier tasks.
+void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int4>& tasks) {
+  tasks.clear();
+  const int R = (int)nt_of_replica.size();
+  std::vector<int> order(R);
+  for (int r = 0; r < R; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return nt_of_replica[x] > nt_of_replica[y]; });
+  int max_nt = 0;
+  for (int v : nt_of_replica) max_nt = std::max(max_nt, v);
+  auto tag = [](int type, int r) { return type | (r << 2); };
+  for (int r : order) {
+    const int nt = nt_of_replica[r];
+    if (nt < 1) continue;
+    tasks.push_back(make_int4(tag(TASK_F, r), 0, 0, 0));
+    for (int i = 1; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, 0, 0));
+  }
+  for (int k = 0; k + 1 < max_nt; ++k)
+    for (int r : order) {
+      const int nt = nt_of_replica[r];
+      if (k + 1 >= nt) continue;
+      tasks.push_back(make_int4(tag(TASK_F, r), k + 1, k + 1, k + 1));
+      for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, k + 1, k + 1));
+      for (int jj = k + 2; jj < nt; ++jj)
+        for (int i = jj; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_U, r), i, jj, k));
+    }
+}
+
+int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
+                          cudaStream_t st) {
+  if (ntasks <= 0) return PBG_OK;
+  const bool f64 = precision == PBG_PREC_FP64;
+  const size_t smem = f64 ? sizeof(double) * batch_smem_elems<double>() : sizeof(float) * batch_smem_elems<float>();
+  static int blocks_per_sm[2] = {-1, -1};
+  static int num_sms = 0;
+  int& bps = blocks_per_sm[f64 ? 0 : 1];
+  if (bps < 0) {
+    int dev;
+    PBG_CUDA_TRY(cudaGetDevice(&dev));
+    PBG_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+    if (f64) {
+      PBG_CUDA_TRY(cudaFuncSetAttribute(chol_batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, chol_batch_kernel<double>, THREADS, smem));
+    } else {
+      PBG_CUDA_TRY(cudaFuncSetAttribute(chol_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, chol_batch_kernel<float>, THREADS, smem));
+    }
+    if (bps < 1) {
+      pbg_set_error_message("batched cholesky kernel does not fit on an SM");
+      bps = -1;
+      return PBG_ERR_CUDA;
+    }
+  }
+  int grid = num_sms * bps;
+  if (grid > ntasks) grid = ntasks;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (f64) PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<double>, reps, tasks, ntasks, ctl));
+  else PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<float>, reps, tasks, ntasks, ctl));
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
 }
 
 }  // namespace pbg

@@ -14,6 +14,7 @@
 // halves the n-set.  The minimum image does not enter the reciprocal part
 // (the phase is periodic), only the real-space images.
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -142,8 +143,9 @@ __device__ __forceinline__ void smith_pair(T sx, T sy, T sz, T cO, T cQ, T alpha
   diag = d + cO * dr;
 }
 
+// One 16 x 16 bead tile (I, J), I >= J, of the tensor described by `a`.
 template <typename T>
-__global__ void __launch_bounds__(THREADS) rpy_tile_kernel(RpyArgs a) {
+__device__ __forceinline__ void rpy_tile_body(const RpyArgs& a, int I, int J) {
   using V2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // layout: out tile [TV][TV+1] T | recip table [n_recip][8] T | real [n_real][4] double |
@@ -159,12 +161,6 @@ __global__ void __launch_bounds__(THREADS) rpy_tile_kernel(RpyArgs a) {
   off = (off + 15) & ~size_t(15);
   V2* s_ph = reinterpret_cast<V2*>(smem_raw + off);
 
-  // Tile (I, J), I >= J, from the linear lower-triangle block index.
-  const int b = blockIdx.x;
-  int I = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-  while ((I + 1) * (I + 2) / 2 <= b) ++I;
-  while (I * (I + 1) / 2 > b) --I;
-  const int J = b - I * (I + 1) / 2;
   const int tid = threadIdx.x;
   const int ti = tid / TB, tj = tid % TB;
   const int i = I * TB + ti, j = J * TB + tj;
@@ -269,6 +265,25 @@ __global__ void __launch_bounds__(THREADS) rpy_tile_kernel(RpyArgs a) {
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(THREADS) rpy_tile_kernel(RpyArgs a) {
+  // Tile (I, J), I >= J, from the linear lower-triangle block index.
+  const int b = blockIdx.x;
+  int I = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+  while ((I + 1) * (I + 2) / 2 <= b) ++I;
+  while (I * (I + 1) / 2 > b) --I;
+  const int J = b - I * (I + 1) / 2;
+  rpy_tile_body<T>(a, I, J);
+}
+
+// Batched build: block b computes tile (work[b].y, work[b].z) of replica work[b].x.
+template <typename T>
+__global__ void __launch_bounds__(THREADS) rpy_batch_kernel(const RpyArgs* __restrict__ args,
+                                                            const int4* __restrict__ work) {
+  const int4 w = work[blockIdx.x];
+  rpy_tile_body<T>(args[w.x], w.y, w.z);
+}
+
 __global__ void positions_from_pairs_kernel(const double* __restrict__ pairs, int n, double* __restrict__ pos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -297,6 +312,30 @@ __global__ void phase_kernel(const double* __restrict__ pos, int n, double L,
     V2 v;
     v.x = c;
     v.y = s;
+    out[(size_t)k * n + bead] = v;
+  }
+}
+
+// Batched phase tables: blockIdx.y = replica, grid-stride over its (k, bead) entries.
+template <typename V2>
+__global__ void phase_batch_kernel(const RpyArgs* __restrict__ args, const double* __restrict__ recip,
+                                   int n_recip) {
+  const RpyArgs& a = args[blockIdx.y];
+  const int n = a.n;
+  const double L = a.L;
+  const double* pos = a.src.pos;
+  V2* out = reinterpret_cast<V2*>(const_cast<void*>(a.phase));
+  const long long total = (long long)n * n_recip;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t / n), bead = (int)(t % n);
+    const double* r = recip + 8 * k;
+    const double ns = r[0] * (pos[3 * bead] / L) + r[1] * (pos[3 * bead + 1] / L) + r[2] * (pos[3 * bead + 2] / L);
+    double sn, cs;
+    sincospi(2.0 * ns, &sn, &cs);
+    V2 v;
+    v.x = cs;
+    v.y = sn;
     out[(size_t)k * n + bead] = v;
   }
 }
@@ -488,6 +527,72 @@ int launch_rpy_tensor(const PairSource& src, const double* pos, const double* ra
   } else {
     PBG_CUDA_TRY(cudaFuncSetAttribute(rpy_tile_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     rpy_tile_kernel<float><<<blocks, THREADS, smem, st>>>(a);
+  }
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+size_t rpy_batch_arg_bytes() { return sizeof(RpyArgs); }
+
+void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool smith, const EwaldTables* t,
+                   double scale, void* M, int ld, void* phase, void* dst) {
+  RpyArgs a{};
+  a.src.pos = pos;
+  a.src.pairs = nullptr;
+  a.src.n = n;
+  a.src.L = L;
+  a.radii = radii;
+  a.M = M;
+  a.L = L;
+  a.scale = scale;
+  a.n = n;
+  a.ld = ld;
+  a.smith = smith ? 1 : 0;
+  if (smith && t) {
+    a.alpha = t->alpha;
+    a.real = t->d_real;
+    a.recip = t->d_recip;
+    a.recip_f = t->d_recip_f;
+    a.n_real = t->n_real;
+    a.n_recip = t->n_recip;
+    for (int c = 0; c < 6; ++c) {
+      a.self_O[c] = t->self_O[c];
+      a.self_Q[c] = t->self_Q[c];
+    }
+    a.phase = phase;
+  }
+  std::memcpy(dst, &a, sizeof(a));
+}
+
+void rpy_batch_work(int replica, int n, std::vector<int4>& work) {
+  const int tiles = (n + TB - 1) / TB;
+  for (int I = 0; I < tiles; ++I)
+    for (int J = 0; J <= I; ++J) work.push_back(make_int4(replica, I, J, 0));
+}
+
+// args: device array of the replicas' argument blocks (rpy_batch_arg);
+// the phase tables are built first (one grid row per replica).
+int launch_rpy_batch(int precision, bool smith, const EwaldTables* t, const void* args, const int4* work,
+                     int nwork, int n_replicas, cudaStream_t st) {
+  if (nwork <= 0) return PBG_OK;
+  const RpyArgs* a = static_cast<const RpyArgs*>(args);
+  if (smith && t && t->n_recip > 0 && n_replicas > 0) {
+    const dim3 grid(16, n_replicas);
+    if (precision == PBG_PREC_FP64) phase_batch_kernel<double2><<<grid, 256, 0, st>>>(a, t->d_recip, t->n_recip);
+    else phase_batch_kernel<float2><<<grid, 256, 0, st>>>(a, t->d_recip, t->n_recip);
+    PBG_CHECK_LAUNCH();
+  }
+  const size_t smem = rpy_smem_bytes(t, precision, smith);
+  if (smem > 227 * 1024) {
+    pbg_set_error_message("Ewald n-set too large for shared memory (%zu bytes)", smem);
+    return PBG_ERR_ARG;
+  }
+  if (precision == PBG_PREC_FP64) {
+    PBG_CUDA_TRY(cudaFuncSetAttribute(rpy_batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rpy_batch_kernel<double><<<nwork, THREADS, smem, st>>>(a, work);
+  } else {
+    PBG_CUDA_TRY(cudaFuncSetAttribute(rpy_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rpy_batch_kernel<float><<<nwork, THREADS, smem, st>>>(a, work);
   }
   PBG_CHECK_LAUNCH();
   return PBG_OK;

@@ -27,23 +27,6 @@ __global__ void pointer_matrix_kernel(const double* __restrict__ pos, int n, dou
   }
 }
 
-// Overlap test of one pair with the reference's axis pre-filter
-// (bead.c:188-216) and minimum-image distance (bead.c:222-260).
-__device__ __forceinline__ bool pair_overlaps(const double* __restrict__ pos,
-                                              const double* __restrict__ radii, int i, int j,
-                                              double L, double thr) {
-  double r[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) r[c] = pos[3 * i + c] - pos[3 * j + c];
-  const double rs = radii[i] + radii[j];
-  const double rs_pbc = L - rs;
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-    if (((r[c] > rs) && (r[c] < rs_pbc)) || ((r[c] < -rs) && (r[c] > -rs_pbc))) return false;
-  const double x = pbg_min_image(r[0], L), y = pbg_min_image(r[1], L), z = pbg_min_image(r[2], L);
-  return sqrt(x * x + y * y + z * z) <= radii[i] + radii[j] + thr;
-}
-
 // Any non-bonded overlapping pair sets *flag.  conn (N*N int32) may be null.
 __global__ void overlap_kernel(const double* __restrict__ pos, const double* __restrict__ radii,
                                int n, double L, double thr, const int* __restrict__ conn,

@@ -1,6 +1,8 @@
 // Internal (C++) interfaces between the pybrown_b200 translation units.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace pbg {
@@ -47,6 +49,23 @@ __device__ __forceinline__ void get_pair_vector(const PairSource& s, int i, int 
 int launch_positions_from_pairs(const double* pairs, int n, double* pos, cudaStream_t st);
 
 // ---- geometry.cu ---------------------------------------------------------
+// Overlap test of one pair with the reference's axis pre-filter
+// (bead.c:188-216) and minimum-image distance (bead.c:222-260).
+__device__ __forceinline__ bool pair_overlaps(const double* __restrict__ pos,
+                                              const double* __restrict__ radii, int i, int j,
+                                              double L, double thr) {
+  double r[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) r[c] = pos[3 * i + c] - pos[3 * j + c];
+  const double rs = radii[i] + radii[j];
+  const double rs_pbc = L - rs;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if (((r[c] > rs) && (r[c] < rs_pbc)) || ((r[c] < -rs) && (r[c] > -rs_pbc))) return false;
+  const double x = pbg_min_image(r[0], L), y = pbg_min_image(r[1], L), z = pbg_min_image(r[2], L);
+  return sqrt(x * x + y * y + z * z) <= radii[i] + radii[j] + thr;
+}
+
 int launch_pointer_matrix(const double* pos, int n, double L, double* rij, cudaStream_t st);
 int launch_overlap(const double* pos, const double* radii, int n, double L, double thr,
                    const int* conn, int* flag, cudaStream_t st);
@@ -100,5 +119,31 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
                        cudaStream_t st);
 size_t spd_inverse_work_bytes(int ld);
 int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st);
+
+// Batched factorisation of many independent matrices (one per replica).
+struct CholRep {
+  void* A;        // ld x ld, padded with the identity beyond n
+  void* invdiag;  // nt x 64 x 64: inv(L_kk) tiles
+  int* upd;       // nt x nt, zero before the launch
+  int* fin;       // nt x nt, zero before the launch
+  int* info;      // zero before the launch
+  int ld, n, nt, pad;
+};
+// Task list of a batch: every replica's F, S and U tasks, interleaved by
+// panel so that no task depends on a later one (task.x = type | replica << 2).
+void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int4>& tasks);
+// ctl: 4 ints (next task, abort, spin failures, error bits), zero before the launch.
+int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
+                          cudaStream_t st);
+
+// Batched RPY / Smith-Ewald tensor build: one argument block per replica and
+// a work list of bead tiles (x = replica, y = I, z = J with I >= J).
+size_t rpy_batch_arg_bytes();
+// Fills the argument block of one replica into `dst` (rpy_batch_arg_bytes() bytes).
+void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool smith, const EwaldTables* t,
+                   double scale, void* M, int ld, void* phase, void* dst);
+void rpy_batch_work(int replica, int n, std::vector<int4>& work);
+int launch_rpy_batch(int precision, bool smith, const EwaldTables* t, const void* args, const int4* work,
+                     int nwork, int n_replicas, cudaStream_t st);
 
 }  // namespace pbg
