@@ -350,7 +350,65 @@ def run_ours(args, torch, dist, rank, world):
         "cpu_baseline": cpu,
         "clocks": results["mixed"]["clocks"],
     }
+    if world == 1 and not args.no_batch:
+        line["batch"] = run_batch_section(args, torch)
+    if world == 1 and not args.no_serve:
+        line["serve"] = run_serve_section(args, torch)
     return line
+
+
+def run_batch_section(args, torch):
+    """256 independent replicas, N uniform in [32, 512] (seed 1), radii uniform
+    in [10, 30], volume fraction 0.05 each, Smith-Ewald m=2 n=4, mixed
+    precision, device noise streams, dt 0.5 ps: one batched step advances all."""
+    from pybrown_b200 import _lib
+    from pybrown_b200.batch import ReplicaBatch
+    from pybrown_b200.serve import place_beads
+    rng = np.random.default_rng(1)
+    Ns = rng.integers(32, 513, size=256)
+    batch = ReplicaBatch(precision="mixed")
+    for k, N in enumerate(Ns):
+        radii = rng.uniform(10.0, 30.0, size=int(N))
+        L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
+        batch.add(place_beads(rng, radii, L), radii, L, seed=k, noise="device")
+    for _ in range(args.warmup):
+        batch.propagate(0.5)
+    torch.cuda.synchronize()
+    launches0 = _lib.lib.pbg_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        batch.propagate(0.5)
+    end.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    launches = (_lib.lib.pbg_launch_count() - launches0) / args.steps
+    beads = int(Ns.sum())
+    batch.close()
+    return {"workload": "256 replicas, N~U[32,512] (seed 1), a~U[10,30], phi=0.05, Smith-Ewald m=2 n=4, "
+                        "mixed, dt=0.5, device Philox noise", "replicas": 256, "beads": beads,
+            "steps": args.steps, "ms_per_step": ms / args.steps,
+            "bead_steps_per_s": beads * args.steps / (ms * 1e-3),
+            "replica_steps_per_s": 256 * args.steps / (ms * 1e-3), "gpu_launches_per_step": launches}
+
+
+def run_serve_section(args, torch):
+    """Continuous batching of a Poisson request stream (50 requests/s, N
+    log-uniform in [16, 2048], radii uniform in [10, 40], phi 0.05, dt 1 ps),
+    scaled to finish in a bench run: a shorter arrival window and fewer steps
+    per request than the full stream (stated in the workload string)."""
+    from pybrown_b200.batch import ReplicaBatch
+    from pybrown_b200.serve import Server, make_stream
+    lo, hi = args.serve_steps
+    stream = make_stream(4, rate=50.0, duration=args.serve_seconds, steps_min=lo, steps_max=hi, dt=1.0)
+    server = Server(ReplicaBatch(precision="mixed"), keep_positions=False)
+    recs, summary = server.run(stream, clock="wall")
+    server.batch.close()
+    summary["workload"] = (f"Poisson 50 req/s for {args.serve_seconds:g} s, N log-U[16,2048], a~U[10,40], "
+                           f"phi=0.05, steps U[{lo},{hi}] (full stream: 60 s, steps U[100,5000]), dt=1, mixed")
+    summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
+    summary["peak_gb"] = summary.pop("peak_bytes") / 1e9
+    return summary
 
 
 def run_reference(args, rank):
@@ -376,6 +434,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas section")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
+    ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving stream")
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=(10, 200), help="steps per request: min max")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -1,0 +1,222 @@
+"""Serving loop: continuous batching of BD-with-HI simulation requests.
+
+Requests (bead configuration, step count, seed) arrive over time.  The loop
+admits a request as soon as it has arrived and its device footprint -- the
+(3N)^2 tensor and factor plus tables and state, ``pbg_batch_footprint`` --
+fits in the memory budget next to the requests already running; admitted
+requests join one ``ReplicaBatch`` and advance together, one batched step at
+a time, so their work overlaps on the device; a request leaves the batch when
+its last step is done, freeing its memory for the next ones.  State stays on
+the device from admission to completion.
+
+Each request draws its noise from its own counter-based device stream keyed
+by its seed, so its result does not depend on what else was running: it is
+the same alone and in the mix.
+
+Completion latency = completion time - arrival time.  ``run`` returns the
+per-request records and a summary with p50/p99 latency and the aggregate
+bead-steps/s over the run.
+
+Two clocks: ``"wall"`` (real time; arrivals are released when the wall clock
+reaches them) and ``"virtual"`` (time advances by ``tick`` per batched step
+and jumps to the next arrival when idle; deterministic, for tests).
+"""
+import collections
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # s since the start of the stream
+    positions: np.ndarray   # N x 3, Angstrom
+    radii: np.ndarray       # N, Angstrom
+    box_length: float       # Angstrom
+    steps: int
+    seed: int
+    dt: float = 1.0         # ps
+    T: float = 293.15
+    viscosity: float = 0.01005
+
+    @property
+    def n_beads(self):
+        return len(self.radii)
+
+
+@dataclass
+class Record:
+    rid: int
+    n_beads: int
+    steps: int
+    arrival: float
+    admitted: float = math.nan
+    completed: float = math.nan
+    positions: np.ndarray = field(default=None, repr=False)
+
+    @property
+    def latency(self):
+        return self.completed - self.arrival
+
+
+def make_stream(seed, rate, duration, n_min=16, n_max=2048, a_lo=10.0, a_hi=40.0, phi=0.05,
+                steps_min=100, steps_max=5000, dt=1.0):
+    """Poisson arrivals at `rate` per second for `duration` seconds; N
+    log-uniform in [n_min, n_max], radii uniform in [a_lo, a_hi], random
+    non-overlapping positions in a periodic cubic box at volume fraction phi,
+    step count uniform in [steps_min, steps_max]."""
+    rng = np.random.default_rng(seed)
+    t, out, rid = 0.0, [], 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        N = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        radii = rng.uniform(a_lo, a_hi, size=N)
+        L = (np.sum(4.0 / 3.0 * np.pi * radii ** 3) / phi) ** (1.0 / 3.0)
+        pos = place_beads(rng, radii, L)
+        steps = int(rng.integers(steps_min, steps_max + 1))
+        out.append(Request(rid, t, pos, radii, float(L), steps, int(rng.integers(0, 2 ** 63)), dt))
+        rid += 1
+    return out
+
+
+def place_beads(rng, radii, L):
+    """Sequential random placement without overlaps (minimum image), on a cell
+    grid so that large N stays fast."""
+    N = len(radii)
+    amax = float(np.max(radii))
+    ncell = max(1, int(L // (2 * amax)))
+    cell = L / ncell
+    grid = collections.defaultdict(list)
+    pos = np.empty((N, 3))
+    for i, a in enumerate(radii):
+        while True:
+            p = rng.uniform(-L / 2, L / 2, size=3)
+            c = np.floor((p + L / 2) / cell).astype(int) % ncell
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        key = ((c[0] + dx) % ncell, (c[1] + dy) % ncell, (c[2] + dz) % ncell)
+                        for j in grid.get(key, ()):
+                            d = p - pos[j]
+                            d -= L * np.round(d / L)
+                            if np.dot(d, d) <= (a + radii[j]) ** 2:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                pos[i] = p
+                grid[tuple(c)].append(i)
+                break
+    return pos
+
+
+class Server:
+    """Continuous-batching request loop over one ReplicaBatch.
+
+    batch: a ReplicaBatch (or an object with add/remove/propagate/positions/
+    footprint); memory_budget: device bytes the admitted requests may take
+    (default: 80 % of the free device memory at start); max_active: optional
+    cap on concurrent requests."""
+
+    def __init__(self, batch=None, memory_budget=None, max_active=None, precision="mixed", keep_positions=True):
+        if batch is None:
+            from .batch import ReplicaBatch
+            batch = ReplicaBatch(precision=precision)
+        self.batch = batch
+        if memory_budget is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info()
+            memory_budget = int(0.8 * free)
+        self.memory_budget = int(memory_budget)
+        self.max_active = max_active
+        self.keep_positions = keep_positions
+
+    def run(self, requests, clock="wall", tick=1e-3):
+        reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        for r in reqs:
+            if self.batch.footprint(r.n_beads) > self.memory_budget:
+                raise ValueError(f"request {r.rid} (N={r.n_beads}) does not fit in the memory budget")
+        pending = collections.deque(reqs)
+        records = {r.rid: Record(r.rid, r.n_beads, r.steps, r.arrival) for r in reqs}
+        active = {}  # slot -> [request, steps left, bytes]
+        used = 0
+        peak_used, peak_active, batched_steps = 0, 0, 0
+        start = time.perf_counter()
+        vnow = 0.0
+
+        def now():
+            return vnow if clock == "virtual" else time.perf_counter() - start
+
+        while pending or active:
+            t = now()
+            # admission: arrived requests, in arrival order, while they fit
+            while pending and pending[0].arrival <= t:
+                r = pending[0]
+                fp = self.batch.footprint(r.n_beads)
+                if used + fp > self.memory_budget or (self.max_active and len(active) >= self.max_active):
+                    break
+                pending.popleft()
+                slot = self.batch.add(r.positions, r.radii, r.box_length, T=r.T, viscosity=r.viscosity,
+                                      seed=r.seed, noise="device")
+                active[slot] = [r, r.steps, fp]
+                used += fp
+                records[r.rid].admitted = now()
+            peak_used = max(peak_used, used)
+            peak_active = max(peak_active, len(active))
+            if not active:
+                # idle until the next arrival
+                nxt = pending[0].arrival
+                if clock == "virtual":
+                    vnow = max(vnow, nxt)
+                else:
+                    time.sleep(max(0.0, nxt - now()))
+                continue
+            dts = {a[0].dt for a in active.values()}
+            if len(dts) != 1:
+                raise ValueError("requests running together must share dt")
+            self.batch.propagate(dts.pop())
+            batched_steps += 1
+            if clock == "virtual":
+                vnow += tick
+            done = []
+            for slot, a in active.items():
+                a[1] -= 1
+                if a[1] == 0:
+                    done.append(slot)
+            if done:
+                t_done = now()
+                for slot in done:
+                    r, _, fp = active.pop(slot)
+                    rec = records[r.rid]
+                    rec.completed = t_done
+                    if self.keep_positions:
+                        rec.positions = self.batch.positions(slot).copy()
+                    self.batch.remove(slot)
+                    used -= fp
+        elapsed = now() if clock == "virtual" else time.perf_counter() - start
+        recs = [records[r.rid] for r in reqs]
+        lat = np.array([x.latency for x in recs]) if recs else np.array([0.0])
+        bead_steps = sum(x.n_beads * x.steps for x in recs)
+        summary = {
+            "requests": len(recs),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "bead_steps_per_s": bead_steps / elapsed if elapsed > 0 else math.inf,
+            "elapsed_s": elapsed,
+            "batched_steps": batched_steps,
+            "peak_active": peak_active,
+            "peak_bytes": peak_used,
+            "memory_budget": self.memory_budget,
+        }
+        return recs, summary
