@@ -831,8 +831,10 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
 template <typename T>
 constexpr int batch_smem_elems() { return 2 * NB * LDA + factor_smem_elems<T>(); }
 
+// Two CTAs per SM in FP32 (127 registers, no spill; more tasks in flight to
+// hide L2 latency), one in FP64 (which would spill).
 template <typename T>
-__global__ void __launch_bounds__(THREADS, 1) chol_batch_kernel(const CholRep* __restrict__ reps,
+__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
                                                                  const int4* __restrict__ tasks, int ntasks,
                                                                  int* ctl) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1030,11 +1032,14 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
 }
 
 
-// Per replica: F(0), S(i, 0); then for each k: F(k+1), S(i, k+1) (i >= k+2),
-// U(i, j, k) (j >= k+2).  F(k+1) and S(., k+1) apply their update with panel
-// k themselves.  The replicas' lists are interleaved block by block, larger
-// matrices first within a block; each replica's own order is kept, so every
-// task depends only on earlier tasks.
+// Per replica: F(0), S(i, 0); then for each k the block F(k+1), U(i, j, k)
+// (j >= k+2), S(i, k+1) (i >= k+2).  F(k+1) and S(., k+1) apply their update
+// with panel k themselves.  Across replicas the blocks are interleaved part by
+// part -- every replica's F(k+1), then every replica's U(., ., k), then every
+// replica's S(., k+1), larger matrices first -- so the solves are fetched
+// after their factorisations had the whole update phase to finish.  F(k+1)
+// and U(., ., k) depend only on block k-1; S(., k+1) on F(k+1) and block k-1:
+// every task depends only on earlier tasks.
 void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int4>& tasks) {
   tasks.clear();
   const int R = (int)nt_of_replica.size();
@@ -1051,15 +1056,19 @@ void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int
     tasks.push_back(make_int4(tag(TASK_F, r), 0, 0, 0));
     for (int i = 1; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, 0, 0));
   }
-  for (int k = 0; k + 1 < max_nt; ++k)
+  for (int k = 0; k + 1 < max_nt; ++k) {
+    for (int r : order)
+      if (k + 1 < nt_of_replica[r]) tasks.push_back(make_int4(tag(TASK_F, r), k + 1, k + 1, k + 1));
     for (int r : order) {
       const int nt = nt_of_replica[r];
-      if (k + 1 >= nt) continue;
-      tasks.push_back(make_int4(tag(TASK_F, r), k + 1, k + 1, k + 1));
-      for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, k + 1, k + 1));
       for (int jj = k + 2; jj < nt; ++jj)
         for (int i = jj; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_U, r), i, jj, k));
     }
+    for (int r : order) {
+      const int nt = nt_of_replica[r];
+      for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, k + 1, k + 1));
+    }
+  }
 }
 
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,

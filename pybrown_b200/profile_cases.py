@@ -2,9 +2,12 @@
 
     python -m pybrown_b200.profile_cases cholesky --order 768 --precision mixed
     python -m pybrown_b200.profile_cases smith --beads 512 --precision fp64
+    python -m pybrown_b200.profile_cases batch --replicas 64 --precision mixed
 
 `cholesky` factors the Smith-Ewald diffusion matrix of a random bead
-configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it.
+configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it;
+`batch` advances a batch of replicas (N uniform in [32, 512], seed 1) by one
+step.
 Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
 time of one launch.
 """
@@ -37,12 +40,15 @@ def main(argv=None):
 
     from . import _lib
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("kernel", choices=("cholesky", "smith"))
+    ap.add_argument("kernel", choices=("cholesky", "smith", "batch"))
+    ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--beads", type=int, default=256)
     ap.add_argument("--order", type=int, default=0, help="cholesky: matrix order (default 3 x beads)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--reps", type=int, default=2)
     a = ap.parse_args(argv)
+    if a.kernel == "batch":
+        return _batch(a, torch)
     prec = _lib.PREC[a.precision]
     dtype = torch.float64 if prec == 0 else torch.float32
     beads = a.order // 3 if a.order else a.beads
@@ -81,6 +87,30 @@ def main(argv=None):
         total += start.elapsed_time(end)
     extra = f" info={int(info.item())}" if a.kernel == "cholesky" else ""
     print(f"{a.kernel} n={n} ({a.precision}): {total / a.reps:.3f} ms per launch{extra}")
+
+
+def _batch(a, torch):
+    from .batch import ReplicaBatch
+    from .serve import place_beads
+    rng = np.random.default_rng(1)
+    Ns = rng.integers(32, 513, size=a.replicas)
+    batch = ReplicaBatch(precision=a.precision)
+    for k, N in enumerate(Ns):
+        radii = rng.uniform(10.0, 30.0, size=int(N))
+        L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
+        batch.add(place_beads(rng, radii, L), radii, L, seed=k, noise="device")
+    batch.propagate(0.5)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(a.reps):
+        start.record()
+        batch.propagate(0.5)
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}): {total / a.reps:.3f} ms per step")
+    batch.close()
 
 
 if __name__ == "__main__":
