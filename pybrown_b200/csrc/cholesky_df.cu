@@ -13,8 +13,8 @@
 //            cores: FP64 DMMA (mma.sync m8n8k4 f64) in the FP64 path,
 //            3xTF32 split products (mma.sync m16n8k8 tf32, hi*hi + hi*lo +
 //            lo*hi, FP32 accumulation) in the mixed path.
-// The diagonal tiles are factored in the precision of the matrix: FP64 in
-// the FP64 path, FP32 in the mixed path.
+// The diagonal tiles are always factored and inverted in FP64; the mixed
+// path (FP32 matrix, 3xTF32 updates) rounds L_kk and inv(L_kk) to FP32 on store.
 //
 // The critical path of the factorisation is F(0), S(1,0), F(1), S(2,1), ...:
 // block 0 (the chain CTA) runs exactly that sequence and keeps what one step
@@ -557,7 +557,9 @@ __device__ __forceinline__ void invert_factor(const T* Lk, const T* Rinv, T* X, 
 // Then L_kk (upper triangle zeroed) goes to global memory and to Lk
 // ([64][LDA] smem), and its inverse is formed in X ([64][LDA] smem) and
 // written to the global invdiag array.  Ends with a CTA barrier.
-template <typename T>
+// T is the arithmetic, S the type of the matrix in global memory (the mixed
+// path factors its FP32 diagonal tiles in FP64 and stores them rounded).
+template <typename T, typename S = T>
 __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T* fs, T* Lk, T* X) {
   constexpr int PB = Strip<T>::PB;
   T* Rinv = fs + 2 * NB * PB;  // [64] 1 / L_jj
@@ -654,19 +656,45 @@ __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T
     // no barrier here: the next panel writes the other strip buffer, and the
     // two barriers of that panel separate these reads from its next reuse
   }
-  T* g = tile<T>(a, k, k);
+  S* g = tile<S>(a, k, k);
 #pragma unroll
   for (int rs = 0; rs < 2; ++rs)
 #pragma unroll
     for (int cs = 0; cs < 8; ++cs) {
       const int r = acc_row(rs), c = acc_col(cs);
       const T v = c <= r ? acc[TileMMA<T>::idx(rs, cs)] : T(0);
-      g[(size_t)r * a.ld + c] = v;
+      g[(size_t)r * a.ld + c] = (S)v;
       Lk[r * LDA + c] = v;
     }
   __syncthreads();
   invert_factor(Lk, Rinv, X, fs);
-  store_tile(X, LDA, reinterpret_cast<T*>(a.invdiag) + (size_t)k * NB * NB, NB);
+  S* inv = reinterpret_cast<S*>(a.invdiag) + (size_t)k * NB * NB;
+  if constexpr (sizeof(S) == sizeof(T)) {
+    store_tile(X, LDA, inv, NB);
+  } else {
+    for (int t = threadIdx.x; t < NB * NB; t += THREADS) inv[t] = (S)X[(t >> 6) * LDA + (t & 63)];
+  }
+}
+
+// F(k) of the mixed path: the FP32 tile in acc (after its last update) is
+// factored and inverted in FP64 (fs64 / Lk64 / X64: double scratch, [64][LDA]
+// tiles), L_kk and inv(L_kk) are stored rounded to FP32, and Xf ([64][LDA]
+// FP32 smem) receives the rounded inverse for the TF32 solves.  The two
+// accumulator layouts map (rs, cs) to the same element.
+__device__ __forceinline__ void factor_tile_fp64(const DFArgs& a, int k, const float acc[16], double* fs64,
+                                                 double* Lk64, double* X64, float* Xf) {
+  double acc64[16];
+#pragma unroll
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs)
+      acc64[TileMMA<double>::idx(rs, cs)] = (double)acc[TileMMA<float>::idx(rs, cs)];
+  factor_tile<double, float>(a, k, acc64, fs64, Lk64, X64);
+  if (Xf)
+    for (int t = threadIdx.x; t < NB * NB; t += THREADS) {
+      const int r = t >> 6, c = t & 63;
+      Xf[r * LDA + c] = (float)X64[r * LDA + c];
+    }
 }
 
 // acc = -(acc + ...) helpers for S: acc = C inv(L_kk)^T with C, X in smem.
@@ -695,11 +723,16 @@ __device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
     for (int cs = 0; cs < 8; ++cs) s[acc_row(rs) * LDA + acc_col(cs)] = acc[TileMMA<T>::idx(rs, cs)];
 }
 
-// Shared memory of the chain CTA (in T elements): four tiles Cp, Cn, X, sA
-// ([64][LDA] each; sA also holds L_kk during F) and the factor scratch.
-// Every piece is a multiple of 16 bytes, so each starts 16-byte aligned.
+// Shared memory of the chain CTA: four T tiles Cp, Cn, X, sA ([64][LDA]
+// each) and the FP64 factor scratch -- in the FP64 path sA also holds L_kk
+// during F and the factor scratch follows it; in the mixed path two more
+// FP64 tiles (L_kk, inverse) come first.  Every piece is a multiple of 16
+// bytes, so each starts 16-byte aligned.
 template <typename T>
-constexpr int chain_smem_elems() { return 4 * NB * LDA + factor_smem_elems<T>(); }
+constexpr size_t chain_smem_bytes() {
+  return sizeof(T) * 4 * NB * LDA + (sizeof(T) == 8 ? 0 : sizeof(double) * 2 * NB * LDA) +
+         sizeof(double) * factor_smem_elems<double>();
+}
 
 // The chain CTA: F(0), S(1, 0), F(1), S(2, 1), ... with L(k, k-1) and
 // inv(L_kk) kept in shared memory from one task to the next.  The last
@@ -712,8 +745,20 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
   T* Cp = reinterpret_cast<T*>(smem);  // L(k, k-1), the previous solve's result
   T* Cn = Cp + NB * LDA;               // this step's solve input / result L(k+1, k)
   T* X = Cn + NB * LDA;                // inv(L_kk)
-  T* sA = X + NB * LDA;                // prefetched A_kk; L_kk at the end of F(k)
-  T* fs = sA + NB * LDA;               // factor scratch
+  T* sA = X + NB * LDA;                // prefetched A_kk; L_kk at the end of F(k) (FP64 path)
+  // FP64 factor scratch: the mixed path keeps its own L_kk and inverse tiles
+  double* Lk64;
+  double* X64;
+  double* fs64;
+  if constexpr (sizeof(T) == 8) {
+    Lk64 = reinterpret_cast<double*>(sA);
+    X64 = reinterpret_cast<double*>(X);
+    fs64 = reinterpret_cast<double*>(sA + NB * LDA);
+  } else {
+    Lk64 = reinterpret_cast<double*>(sA + NB * LDA);
+    X64 = Lk64 + NB * LDA;
+    fs64 = X64 + NB * LDA;
+  }
   const int nt = a.nt;
   bool pf = false;  // A_kk prefetched into sA
   for (int k = 0; k < nt; ++k) {
@@ -735,7 +780,8 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
       load_acc(tile<T>(a, 0, 0), a.ld, acc);
     }
     TRACE(1, a.ntasks + 2 * k);
-    factor_tile<T>(a, k, acc, fs, sA, X);
+    if constexpr (sizeof(T) == 8) factor_tile<double>(a, k, acc, fs64, Lk64, X64);
+    else factor_tile_fp64(a, k, acc, fs64, Lk64, X64, X);
     publish(a.fin + k * nt + k, 1);
     TRACE(2, a.ntasks + 2 * k);
     if (k + 1 == nt) return;
@@ -826,13 +872,18 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
 }
 
 // Batched factorisation: every task comes from the shared list (there is no
-// chain CTA); F(k) applies its last update itself.  Shared memory: two tiles
-// (sA / L_kk, sB / inv(L_kk)) and the factor scratch.
+// chain CTA); F(k) applies its last update itself.  Shared memory: two T
+// tiles (sA, sB) for the updates and solves; F uses two FP64 tiles (L_kk,
+// inverse) over the same bytes and the FP64 factor scratch after them.
 template <typename T>
-constexpr int batch_smem_elems() { return 2 * NB * LDA + factor_smem_elems<T>(); }
+constexpr size_t batch_smem_bytes() {
+  return sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>());
+}
 
-// Two CTAs per SM in FP32 (127 registers, no spill; more tasks in flight to
-// hide L2 latency), one in FP64 (which would spill).
+// Two CTAs per SM in the mixed path: a second task in flight per SM hides
+// L2 latency (measured 9.8 ms against 12.4 ms for a 256-replica step at one
+// CTA per SM), at the price of a small register spill in the FP64 factor of
+// the F tasks.  One CTA per SM in the FP64 path.
 template <typename T>
 __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
                                                                  const int4* __restrict__ tasks, int ntasks,
@@ -841,7 +892,9 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
   __shared__ int s_task, s_ok;
   T* sA = reinterpret_cast<T*>(smem);
   T* sB = sA + NB * LDA;
-  T* fs = sB + NB * LDA;
+  double* Lk64 = reinterpret_cast<double*>(smem);
+  double* X64 = Lk64 + NB * LDA;
+  double* fs64 = X64 + NB * LDA;
   while (true) {
     if (threadIdx.x == 0) s_task = ld_acquire(ctl + 1) ? ntasks : atomicAdd(ctl, 1);
     __syncthreads();
@@ -884,7 +937,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
         load_acc(tile<T>(a, i, col), a.ld, acc);
       }
       if (type == TASK_F) {
-        factor_tile<T>(a, col, acc, fs, sA, sB);
+        if constexpr (sizeof(T) == 8) factor_tile<double>(a, col, acc, fs64, Lk64, X64);
+        else factor_tile_fp64(a, col, acc, fs64, Lk64, X64, nullptr);
       } else {
         if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
         stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);
@@ -941,7 +995,7 @@ int get_task_table(int nt, const int4** out, int* count) {
 
 template <typename T>
 size_t df_smem_bytes() {
-  return sizeof(T) * (size_t)chain_smem_elems<T>();
+  return chain_smem_bytes<T>();
 }
 
 template <typename T>
@@ -1075,7 +1129,7 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
                           cudaStream_t st) {
   if (ntasks <= 0) return PBG_OK;
   const bool f64 = precision == PBG_PREC_FP64;
-  const size_t smem = f64 ? sizeof(double) * batch_smem_elems<double>() : sizeof(float) * batch_smem_elems<float>();
+  const size_t smem = f64 ? batch_smem_bytes<double>() : batch_smem_bytes<float>();
   static int blocks_per_sm[2] = {-1, -1};
   static int num_sms = 0;
   int& bps = blocks_per_sm[f64 ? 0 : 1];
