@@ -102,6 +102,20 @@ __device__ __forceinline__ void smith_pair(T sx, T sy, T sz, T cO, T cQ, T alpha
   const T q1 = (T)2 / sqrt_pi;
   const T q2 = (T)4 * alpha2 * alpha / sqrt_pi;
   T d = 0;
+  // FP32: the image sum is compensated (Kahan): comp holds minus the
+  // low-order bits lost so far; FP64 keeps the reference's plain summation.
+  constexpr bool kahan = sizeof(T) == 4;
+  T comp[7] = {0, 0, 0, 0, 0, 0, 0};
+  auto add = [&](T& s, T& c, T v) {
+    if constexpr (kahan) {
+      const T yv = v - c;
+      const T t = s + yv;
+      c = (t - s) - yv;
+      s = t;
+    } else {
+      s += v;
+    }
+  };
 #pragma unroll 1
   for (int m = 0; m < n_real; ++m) {
     const T x = sx + (T)s_real[4 * m + 0];
@@ -114,14 +128,19 @@ __device__ __forceinline__ void smith_pair(T sx, T sy, T sz, T cO, T cQ, T alpha
     const T e = d_exp(-alpha2 * l2);
     const T W = ec + q1 * alpha * l * e;
     const T il3 = il * il * il;
-    d += cO * ec * il + cQ * W * il3;
+    add(d, comp[6], cO * ec * il + cQ * W * il3);
     const T oc = (cO * (ec * il + o_real * e) - cQ * ((T)3 * W * il3 + q2 * e)) / l2;
-    acc[0] += oc * x * x;
-    acc[1] += oc * y * y;
-    acc[2] += oc * z * z;
-    acc[3] += oc * x * y;
-    acc[4] += oc * x * z;
-    acc[5] += oc * y * z;
+    add(acc[0], comp[0], oc * x * x);
+    add(acc[1], comp[1], oc * y * y);
+    add(acc[2], comp[2], oc * z * z);
+    add(acc[3], comp[3], oc * x * y);
+    add(acc[4], comp[4], oc * x * z);
+    add(acc[5], comp[5], oc * y * z);
+  }
+  if constexpr (kahan) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] -= comp[c];
+    d -= comp[6];
   }
   T dr = 0;
 #pragma unroll 2
