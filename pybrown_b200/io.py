@@ -122,3 +122,10 @@ def truncate_output_file_during_restart(filename, line):
             dst.write(ln)
     if os.path.exists(tmp):
         os.remove(tmp)
+
+
+def write_to_enr_file(enr_file, j, dt, E, energy_unit_string):
+    """output.py:108-118."""
+    if j == 0:
+        enr_file.write("time/ps energy/{}\n".format(energy_unit_string))
+    enr_file.write("{} {}\n".format(j * dt, E))
