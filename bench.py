@@ -254,6 +254,14 @@ def cpu_reference_steps(N, steps, warmup, threads=None):
     return steps / dt, cores, kind, sample
 
 
+# DRAM bytes (read + write) of one mixed factorisation of the N=1024 matrix,
+# from one ncu capture of the same kernel on the same order:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:chol_df -c 1 --clock-control none \
+#       python -m pybrown_b200.profile_cases cholesky --order 3072 --precision mixed
+# (19,651,072 + 2,610,432 B); re-measure when the factorisation changes.
+CHOL_MIXED_TRAFFIC_BYTES = 19651072 + 2610432
+
+
 def run_ours(args, torch, dist, rank, world):
     from pybrown_b200 import _lib
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -344,9 +352,11 @@ def run_ours(args, torch, dist, rank, world):
         "gpu_launches": results["mixed"]["launches"],
         "roofline": {"kernel": "cholesky (mixed)", "bound": "tensor", "achieved": achieved_tflops,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                     "frac": achieved_tflops / peaks["bf16_tflops"], "traffic": None,
+                     "frac": achieved_tflops / peaks["bf16_tflops"], "traffic": CHOL_MIXED_TRAFFIC_BYTES,
                      "note": f"(3N)^3/3 = {flops:.3e} flop per factorisation in {chol_ms:.3f} ms; "
-                             f"peak is the {peak_kind} dense bf16 figure"},
+                             f"peak is the {peak_kind} dense bf16 figure; the factorisation is bound "
+                             f"by its 48-panel dependency chain, not by a throughput unit; traffic "
+                             f"(bytes per launch) from one ncu capture of the same order"},
         "cpu_baseline": cpu,
         "clocks": results["mixed"]["clocks"],
     }
