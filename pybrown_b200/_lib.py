@@ -121,6 +121,7 @@ _SIGNATURES = {
     "pbg_batch_step_attempt": (_i, [_vp, _vp, _vp, _vp]),
     "pbg_batch_step_end": (_i, [_vp, _vp, _vp]),
     "pbg_batch_get_matrix": (_i, [_vp, _i, _i, _vp]),
+    "pbg_selftest_wait_expiry": (_i, [_ll, _ip, ctypes.POINTER(ctypes.c_uint)]),
 }
 
 

@@ -62,6 +62,7 @@ struct DFArgs {
   int* info;
   void* invdiag; // nt * 64 * 64 (T): inv(L_kk), row-major tiles
   unsigned* err;
+  long long spin_limit;  // polls before a wait gives up
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -108,7 +109,7 @@ __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* ta
       long long it = 0;
       while (ld_acquire(flags[q]) < targets[q]) {
         if (ld_acquire(a.ctl + 1)) { ok = 0; break; }
-        if (++it > SPIN_LIMIT) {
+        if (++it > a.spin_limit) {
           atomicExch(a.ctl + 1, 1);
           atomicAdd(a.ctl + 2, 1);
           atomicOr(a.err, PBG_DEV_ERR_BARRIER);
@@ -917,6 +918,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
     a.info = R.info;
     a.invdiag = R.invdiag;
     a.err = reinterpret_cast<unsigned*>(ctl + 3);
+    a.spin_limit = SPIN_LIMIT;
     const int nt = a.nt;
     T acc[16];
     if (type == TASK_U) {
@@ -998,13 +1000,20 @@ size_t df_smem_bytes() {
   return chain_smem_bytes<T>();
 }
 
+// tasks_override / spin_limit: only for the wait-expiry self-test.
 template <typename T>
-int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned* err, cudaStream_t st) {
+int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned* err, cudaStream_t st,
+              const int4* tasks_override = nullptr, int ntasks_override = 0, long long spin_limit = SPIN_LIMIT) {
   const int nt = ld / NB;
   const int4* tasks = nullptr;
   int ntasks = 0;
-  int rc = get_task_table(nt, &tasks, &ntasks);
-  if (rc) return rc;
+  if (tasks_override) {
+    tasks = tasks_override;
+    ntasks = ntasks_override;
+  } else {
+    int rc = get_task_table(nt, &tasks, &ntasks);
+    if (rc) return rc;
+  }
   const size_t smem = df_smem_bytes<T>();
   static int max_blocks_per_sm = -1;
   static int num_sms = 0;
@@ -1037,6 +1046,7 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
   args.info = info;
   args.invdiag = invdiag;
   args.err = err;
+  args.spin_limit = spin_limit;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(THREADS);
@@ -1053,6 +1063,84 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
 }
 
 }  // namespace
+
+// Self-test of the bounded waits (no counterpart in the reference): factors a
+// 192 x 192 SPD matrix with a task list from which the host drops the update
+// U(2,2,0), so the wait of F(2) for it can never be satisfied.  The wait
+// gives up after spin_limit polls; the launch must end with info = -1 and the
+// barrier error bit, the device must stay usable, and a normal
+// factorisation right after must succeed.  Returns PBG_OK when all of that
+// holds; *info_out and *err_out receive what the aborted launch reported.
+extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(long long spin_limit, int* info_out,
+                                                                                unsigned* err_out) {
+  using namespace pbg;
+  const int n = 192, ld = 192, nt = 3;
+  if (spin_limit < 1 || spin_limit > (1LL << 24)) return PBG_ERR_ARG;
+  const int4* full = nullptr;
+  int nfull = 0;
+  int rc = get_task_table(nt, &full, &nfull);
+  if (rc) return rc;
+  std::vector<int4> tasks(nfull);
+  PBG_CUDA_TRY(cudaMemcpy(tasks.data(), full, nfull * sizeof(int4), cudaMemcpyDeviceToHost));
+  const auto dropped = std::remove_if(tasks.begin(), tasks.end(), [](const int4& t) {
+    return t.x == TASK_U && t.y == 2 && t.z == 2 && t.w == 0;
+  });
+  if (dropped == tasks.end()) return PBG_ERR_STATE;
+  tasks.erase(dropped, tasks.end());
+  std::vector<double> h((size_t)ld * ld, 0.0);
+  for (int i = 0; i < n; ++i) {
+    h[(size_t)i * ld + i] = 4.0;
+    if (i > 0) h[(size_t)i * ld + i - 1] = h[(size_t)(i - 1) * ld + i] = 1.0;
+  }
+  double *A = nullptr, *inv = nullptr;
+  int4* dt = nullptr;
+  int* ints = nullptr;
+  const size_t nints = 3 + 2 * (size_t)nt * nt + 2;
+  bool ok = cudaMalloc(&A, h.size() * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&inv, (size_t)nt * NB * NB * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&dt, tasks.size() * sizeof(int4)) == cudaSuccess &&
+            cudaMalloc(&ints, nints * sizeof(int)) == cudaSuccess;
+  int result = PBG_OK;
+  if (!ok) {
+    cudaGetLastError();
+    result = PBG_ERR_NOMEM;
+  } else {
+    int* info = ints + nints - 2;
+    unsigned* err = reinterpret_cast<unsigned*>(ints + nints - 1);
+    int hinfo = 0;
+    unsigned herr = 0;
+    cudaMemcpy(A, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(dt, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    cudaMemset(err, 0, sizeof(unsigned));
+    result = launch_df<double>(A, n, ld, info, inv, ints, err, 0, dt, (int)tasks.size(), spin_limit);
+    if (result == PBG_OK && cudaDeviceSynchronize() != cudaSuccess) result = PBG_ERR_CUDA;
+    if (result == PBG_OK) {
+      cudaMemcpy(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost);
+      cudaMemcpy(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+      if (info_out) *info_out = hinfo;
+      if (err_out) *err_out = herr;
+      if (hinfo != -1 || !(herr & PBG_DEV_ERR_BARRIER)) result = PBG_ERR_STATE;
+    }
+    if (result == PBG_OK) {
+      // the context is still usable: the full task list factors the matrix
+      cudaMemcpy(A, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemset(err, 0, sizeof(unsigned));
+      result = launch_df<double>(A, n, ld, info, inv, ints, err, 0);
+      if (result == PBG_OK && cudaDeviceSynchronize() != cudaSuccess) result = PBG_ERR_CUDA;
+      if (result == PBG_OK) {
+        cudaMemcpy(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost);
+        if (hinfo != 0) result = PBG_ERR_STATE;
+      }
+    }
+  }
+  if (A) cudaFree(A);
+  if (inv) cudaFree(inv);
+  if (dt) cudaFree(dt);
+  if (ints) cudaFree(ints);
+  if (result != PBG_OK && result != PBG_ERR_CUDA)
+    pbg_set_error_message("wait-expiry self-test: the aborted launch or the follow-up factorisation misbehaved");
+  return result;
+}
 
 #ifdef PBG_TASK_TRACE
 extern "C" __attribute__((visibility("default"))) int pbg_task_trace(long long* host, int ntasks) {
