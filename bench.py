@@ -415,7 +415,9 @@ def run_serve_section(args, torch):
     recs, summary = server.run(stream, clock="wall")
     server.batch.close()
     summary["workload"] = (f"Poisson 50 req/s for {args.serve_seconds:g} s, N log-U[16,2048], a~U[10,40], "
-                           f"phi=0.05, steps U[{lo},{hi}] (full stream: 60 s, steps U[100,5000]), dt=1, mixed")
+                           f"phi=0.05, steps U[{lo},{hi}] (full stream: 60 s, steps U[100,5000], about 40x "
+                           f"the work per request), dt=1, mixed, device noise")
+    summary["offered_bead_steps_per_s"] = sum(r.n_beads * r.steps for r in stream) / args.serve_seconds
     summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
     summary["peak_gb"] = summary.pop("peak_bytes") / 1e9
     return summary
@@ -447,7 +449,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving stream")
-    ap.add_argument("--serve-steps", type=int, nargs=2, default=(10, 200), help="steps per request: min max")
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=(5, 30), help="steps per request: min max")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

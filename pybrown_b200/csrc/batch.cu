@@ -35,6 +35,16 @@ struct BatchReplica {
   void *D = nullptr, *B = nullptr, *invdiag = nullptr, *phase = nullptr;
   bool has_force = false;
   unsigned long long seed = 0, draws = 0;
+  // this replica's Cholesky task list on the device (built once, when added)
+  int4* tasks = nullptr;
+  std::vector<int> seg_start;
+};
+
+// One piece of a merged task list: `count` tasks of replica `replica`.
+struct GatherSeg {
+  const int4* src;
+  long long dst;
+  int count, replica;
 };
 
 // What the vector kernels need of one replica.
@@ -72,6 +82,11 @@ struct pbg_batch {
   pbg::CholRep* d_chol = nullptr;
   int4* d_tasks = nullptr;
   int ntasks = 0;
+  pbg::GatherSeg* d_segs = nullptr;
+  int4* d_eparts = nullptr;  // per replica: tiles per edge, offset in the Ewald work list
+  // capacities (bytes) of the grow-only arrays above
+  size_t cap_reps = 0, cap_rpy = 0, cap_ework = 0, cap_chol = 0, cap_tasks = 0, cap_segs = 0, cap_eparts = 0,
+         cap_flags = 0;
   int* d_flags = nullptr;  // [4 ctl][per replica: upd nt^2, fin nt^2][R infos]
   size_t flag_ints = 0;
   int* d_info = nullptr;
@@ -243,7 +258,7 @@ inline size_t elem_size(int precision) { return precision == PBG_PREC_FP64 ? 8 :
 
 void free_replica(BatchReplica* r) {
   if (!r) return;
-  void* bufs[] = {r->pos, r->radii, r->force, r->U, r->xi, r->D, r->B, r->invdiag, r->phase};
+  void* bufs[] = {r->pos, r->radii, r->force, r->U, r->xi, r->D, r->B, r->invdiag, r->phase, r->tasks};
   for (void* p : bufs)
     if (p) cudaFree(p);
   delete r;
@@ -255,27 +270,68 @@ void free_dev(P*& p) {
   p = nullptr;
 }
 
-// Rebuilds the device descriptors and work lists of the current membership.
-int rebuild(pbg_batch* b) {
+// Device array of at least `bytes`, kept between rebuilds (grow only).
+template <typename P>
+int ensure(P*& p, size_t& cap, size_t bytes) {
+  if (bytes <= cap && p) return PBG_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  const size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+  if (cudaMalloc((void**)&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    pbg_set_error_message("out of device memory for the batch descriptors (%zu bytes)", want);
+    return PBG_ERR_NOMEM;
+  }
+  cap = want;
+  return PBG_OK;
+}
+
+// Merged task list: copies every segment and writes its replica index.
+__global__ void gather_tasks_kernel(const GatherSeg* __restrict__ segs, int nseg, int4* __restrict__ out) {
+  for (int s = blockIdx.x; s < nseg; s += gridDim.x) {
+    const GatherSeg g = segs[s];
+    for (int t = threadIdx.x; t < g.count; t += blockDim.x) {
+      int4 v = g.src[t];
+      v.x = (v.x & 3) | (g.replica << 2);
+      out[g.dst + t] = v;
+    }
+  }
+}
+
+// Ewald work list: replica q's lower-triangle bead tiles (I, J), I >= J, in
+// row order, at parts[q].y; parts[q].x = tiles per edge.
+__global__ void ewald_work_kernel(const int4* __restrict__ parts, int4* __restrict__ out) {
+  const int q = blockIdx.y;
+  const int T = parts[q].x;
+  const long long off = parts[q].y;
+  const int total = T * (T + 1) / 2;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    out[off + t] = make_int4(q, I, t - I * (I + 1) / 2, 0);
+  }
+}
+
+// Rebuilds the device descriptors and work lists of the current membership:
+// small per-replica descriptors from the host, the task and tile work lists
+// assembled on the device from each replica's cached list.
+int rebuild(pbg_batch* b, cudaStream_t st) {
   b->active.clear();
   for (int s = 0; s < (int)b->slots.size(); ++s)
     if (b->slots[s]) b->active.push_back(s);
   const int R = (int)b->active.size();
-  free_dev(b->d_reps);
-  free_dev(b->d_rpy);
-  free_dev(b->d_ework);
-  free_dev(b->d_chol);
-  free_dev(b->d_tasks);
-  free_dev(b->d_flags);
   b->n_ework = b->ntasks = 0;
   if ((size_t)R > b->cap || !b->d_ovl) {
+    PBG_CUDA_TRY(cudaDeviceSynchronize());
     free_dev(b->d_ovl);
     free_dev(b->d_mask);
     free_dev(b->d_stream);
     if (b->h_ovl) cudaFreeHost(b->h_ovl);
     if (b->h_info) cudaFreeHost(b->h_info);
     b->h_ovl = b->h_info = nullptr;
-    b->cap = std::max<size_t>(R, 16);
+    b->cap = std::max<size_t>(2 * R, 16);
     PBG_CUDA_TRY(cudaMalloc(&b->d_ovl, b->cap * sizeof(int)));
     PBG_CUDA_TRY(cudaMalloc(&b->d_mask, b->cap));
     PBG_CUDA_TRY(cudaMalloc(&b->d_stream, 2 * b->cap * sizeof(unsigned long long)));
@@ -287,23 +343,30 @@ int rebuild(pbg_batch* b) {
     b->dirty = false;
     return PBG_OK;
   }
+  // grow-only arrays: the kernels of earlier steps must be done with them
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
   std::vector<BatchDev> reps(R);
   std::vector<unsigned char> rpy(R * rpy_batch_arg_bytes());
-  std::vector<int4> ework;
-  std::vector<int> nts(R);
-  size_t flag_ints = 4;
+  std::vector<int4> eparts(R);
+  size_t flag_ints = 4, n_ework = 0, ntasks = 0;
   std::vector<size_t> flag_off(R);
+  int max_seg = 0;
   for (int q = 0; q < R; ++q) {
     const BatchReplica* r = b->slots[b->active[q]];
     flag_off[q] = flag_ints;
     flag_ints += 2 * (size_t)r->nt * r->nt;
-    nts[q] = r->nt;
     b->max_n = std::max(b->max_n, r->n);
+    const int T = (r->N + 15) / 16;
+    eparts[q] = make_int4(T, (int)n_ework, 0, 0);
+    n_ework += (size_t)T * (T + 1) / 2;
+    ntasks += r->seg_start.empty() ? 0 : r->seg_start.back();
+    max_seg = std::max(max_seg, (int)r->seg_start.size() - 1);
   }
   const size_t info_off = flag_ints;
   flag_ints += R;
   b->flag_ints = flag_ints;
-  PBG_CUDA_TRY(cudaMalloc(&b->d_flags, flag_ints * sizeof(int)));
+  int rc;
+  if ((rc = ensure(b->d_flags, b->cap_flags, flag_ints * sizeof(int)))) return rc;
   b->d_info = b->d_flags + info_off;
   std::vector<CholRep> chol(R);
   const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
@@ -328,7 +391,6 @@ int rebuild(pbg_batch* b) {
     d.pad = 0;
     rpy_batch_arg(r->pos, r->radii, r->N, r->p.box_length, smith, b->tables, r->scale, r->D, r->ld, r->phase,
                   rpy.data() + q * rpy_batch_arg_bytes());
-    rpy_batch_work(q, r->N, ework);
     CholRep& c = chol[q];
     c.A = r->B;
     c.invdiag = r->invdiag;
@@ -340,21 +402,47 @@ int rebuild(pbg_batch* b) {
     c.nt = r->nt;
     c.pad = 0;
   }
-  std::vector<int4> tasks;
-  cholesky_batch_tasks(nts, tasks);
-  PBG_CUDA_TRY(cudaMalloc(&b->d_reps, R * sizeof(BatchDev)));
-  PBG_CUDA_TRY(cudaMalloc(&b->d_rpy, rpy.size()));
-  PBG_CUDA_TRY(cudaMalloc(&b->d_ework, ework.size() * sizeof(int4)));
-  PBG_CUDA_TRY(cudaMalloc(&b->d_chol, R * sizeof(CholRep)));
-  PBG_CUDA_TRY(cudaMalloc(&b->d_tasks, std::max<size_t>(tasks.size(), 1) * sizeof(int4)));
-  PBG_CUDA_TRY(cudaMemcpy(b->d_reps, reps.data(), R * sizeof(BatchDev), cudaMemcpyHostToDevice));
-  PBG_CUDA_TRY(cudaMemcpy(b->d_rpy, rpy.data(), rpy.size(), cudaMemcpyHostToDevice));
-  PBG_CUDA_TRY(cudaMemcpy(b->d_ework, ework.data(), ework.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  PBG_CUDA_TRY(cudaMemcpy(b->d_chol, chol.data(), R * sizeof(CholRep), cudaMemcpyHostToDevice));
-  if (!tasks.empty())
-    PBG_CUDA_TRY(cudaMemcpy(b->d_tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  b->n_ework = (int)ework.size();
-  b->ntasks = (int)tasks.size();
+  // merge order: segment number, then larger matrices first (see cholesky_df.cu)
+  std::vector<int> order(R);
+  for (int q = 0; q < R; ++q) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return b->slots[b->active[x]]->nt > b->slots[b->active[y]]->nt;
+  });
+  std::vector<GatherSeg> segs;
+  long long dst = 0;
+  for (int sg = 0; sg < max_seg; ++sg)
+    for (int q : order) {
+      const BatchReplica* r = b->slots[b->active[q]];
+      if (sg + 1 >= (int)r->seg_start.size()) continue;
+      const int count = r->seg_start[sg + 1] - r->seg_start[sg];
+      if (count <= 0) continue;
+      segs.push_back(GatherSeg{r->tasks + r->seg_start[sg], dst, count, q});
+      dst += count;
+    }
+  if ((rc = ensure(b->d_reps, b->cap_reps, R * sizeof(BatchDev))) ||
+      (rc = ensure(b->d_rpy, b->cap_rpy, rpy.size())) ||
+      (rc = ensure(b->d_ework, b->cap_ework, n_ework * sizeof(int4))) ||
+      (rc = ensure(b->d_chol, b->cap_chol, R * sizeof(CholRep))) ||
+      (rc = ensure(b->d_tasks, b->cap_tasks, std::max<size_t>(ntasks, 1) * sizeof(int4))) ||
+      (rc = ensure(b->d_segs, b->cap_segs, std::max<size_t>(segs.size(), 1) * sizeof(GatherSeg))) ||
+      (rc = ensure(b->d_eparts, b->cap_eparts, R * sizeof(int4))))
+    return rc;
+  // pageable sources: each copy is staged before the call returns
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_reps, reps.data(), R * sizeof(BatchDev), cudaMemcpyHostToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_rpy, rpy.data(), rpy.size(), cudaMemcpyHostToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_chol, chol.data(), R * sizeof(CholRep), cudaMemcpyHostToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_eparts, eparts.data(), R * sizeof(int4), cudaMemcpyHostToDevice, st));
+  if (!segs.empty()) {
+    PBG_CUDA_TRY(cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(GatherSeg), cudaMemcpyHostToDevice,
+                                 st));
+    gather_tasks_kernel<<<(int)std::min<size_t>(segs.size(), 148 * 16), 256, 0, st>>>(b->d_segs, (int)segs.size(),
+                                                                                      b->d_tasks);
+    PBG_CHECK_LAUNCH();
+  }
+  ewald_work_kernel<<<dim3(8, R), 256, 0, st>>>(b->d_eparts, b->d_ework);
+  PBG_CHECK_LAUNCH();
+  b->n_ework = (int)n_ework;
+  b->ntasks = (int)dst;
   b->dirty = false;
   return PBG_OK;
 }
@@ -425,6 +513,8 @@ PBG_API int pbg_batch_destroy(pbg_batch* b) {
   free_dev(b->d_ework);
   free_dev(b->d_chol);
   free_dev(b->d_tasks);
+  free_dev(b->d_segs);
+  free_dev(b->d_eparts);
   free_dev(b->d_flags);
   free_dev(b->d_ovl);
   free_dev(b->d_mask);
@@ -475,6 +565,12 @@ PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, 
             cudaMalloc(&r->invdiag, (size_t)r->nt * PBG_TILE * PBG_TILE * es) == cudaSuccess;
   const size_t ph = phase_scratch_bytes(r->N, b->tables, b->precision);
   if (ok && ph) ok = cudaMalloc(&r->phase, ph) == cudaSuccess;
+  std::vector<int4> tasks;
+  cholesky_replica_tasks(r->nt, tasks, r->seg_start);
+  if (ok && !tasks.empty()) {
+    ok = cudaMalloc(&r->tasks, tasks.size() * sizeof(int4)) == cudaSuccess &&
+         cudaMemcpy(r->tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice) == cudaSuccess;
+  }
   if (!ok) {
     cudaGetLastError();
     free_replica(r);
@@ -569,7 +665,7 @@ PBG_API int pbg_batch_fill_noise(pbg_batch* b, const unsigned char* mask, void* 
   if (!b) return PBG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
-  if (b->dirty && (rc = rebuild(b))) return rc;
+  if (b->dirty && (rc = rebuild(b, st))) return rc;
   const int R = (int)b->active.size();
   if (!R) return PBG_OK;
   int count = 0;
@@ -604,7 +700,7 @@ PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int chole
   }
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
-  if (b->dirty && (rc = rebuild(b))) return rc;
+  if (b->dirty && (rc = rebuild(b, st))) return rc;
   b->dt = dt;
   const int R = (int)b->active.size();
   if (!R) {

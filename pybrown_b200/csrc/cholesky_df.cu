@@ -1174,43 +1174,34 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
 }
 
 
-// Per replica: F(0), S(i, 0); then for each k the block F(k+1), U(i, j, k)
-// (j >= k+2), S(i, k+1) (i >= k+2).  F(k+1) and S(., k+1) apply their update
-// with panel k themselves.  Across replicas the blocks are interleaved part by
-// part -- every replica's F(k+1), then every replica's U(., ., k), then every
-// replica's S(., k+1), larger matrices first -- so the solves are fetched
-// after their factorisations had the whole update phase to finish.  F(k+1)
-// and U(., ., k) depend only on block k-1; S(., k+1) on F(k+1) and block k-1:
-// every task depends only on earlier tasks.
-void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int4>& tasks) {
+// One replica's tasks in its own order, cut into segments: segment 0 =
+// F(0), S(i, 0); then for each k three segments F(k+1) | U(i, j, k) (j >= k+2)
+// | S(i, k+1) (i >= k+2).  F(k+1) and S(., k+1) apply their update with panel
+// k themselves.  seg_start holds 1 + 3(nt-1) segment starts and the end.
+// A batch merges the replicas' lists segment number by segment number (all
+// replicas' segment s, larger matrices first, then segment s+1): every
+// replica's F(k+1), then every replica's U(., ., k), then every replica's
+// S(., k+1), so the solves are fetched after their factorisations had the
+// whole update phase to finish.  F(k+1) and U(., ., k) depend only on block
+// k-1; S(., k+1) on F(k+1) and block k-1: every task depends only on earlier
+// tasks.  The tasks carry replica tag 0; the merge writes the replica index.
+void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start) {
   tasks.clear();
-  const int R = (int)nt_of_replica.size();
-  std::vector<int> order(R);
-  for (int r = 0; r < R; ++r) order[r] = r;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int x, int y) { return nt_of_replica[x] > nt_of_replica[y]; });
-  int max_nt = 0;
-  for (int v : nt_of_replica) max_nt = std::max(max_nt, v);
-  auto tag = [](int type, int r) { return type | (r << 2); };
-  for (int r : order) {
-    const int nt = nt_of_replica[r];
-    if (nt < 1) continue;
-    tasks.push_back(make_int4(tag(TASK_F, r), 0, 0, 0));
-    for (int i = 1; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, 0, 0));
+  seg_start.clear();
+  if (nt < 1) return;
+  seg_start.push_back(0);
+  tasks.push_back(make_int4(TASK_F, 0, 0, 0));
+  for (int i = 1; i < nt; ++i) tasks.push_back(make_int4(TASK_S, i, 0, 0));
+  for (int k = 0; k + 1 < nt; ++k) {
+    seg_start.push_back((int)tasks.size());
+    tasks.push_back(make_int4(TASK_F, k + 1, k + 1, k + 1));
+    seg_start.push_back((int)tasks.size());
+    for (int jj = k + 2; jj < nt; ++jj)
+      for (int i = jj; i < nt; ++i) tasks.push_back(make_int4(TASK_U, i, jj, k));
+    seg_start.push_back((int)tasks.size());
+    for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(TASK_S, i, k + 1, k + 1));
   }
-  for (int k = 0; k + 1 < max_nt; ++k) {
-    for (int r : order)
-      if (k + 1 < nt_of_replica[r]) tasks.push_back(make_int4(tag(TASK_F, r), k + 1, k + 1, k + 1));
-    for (int r : order) {
-      const int nt = nt_of_replica[r];
-      for (int jj = k + 2; jj < nt; ++jj)
-        for (int i = jj; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_U, r), i, jj, k));
-    }
-    for (int r : order) {
-      const int nt = nt_of_replica[r];
-      for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(tag(TASK_S, r), i, k + 1, k + 1));
-    }
-  }
+  seg_start.push_back((int)tasks.size());
 }
 
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,

@@ -129,9 +129,10 @@ struct CholRep {
   int* info;      // zero before the launch
   int ld, n, nt, pad;
 };
-// Task list of a batch: every replica's F, S and U tasks, interleaved by
-// panel so that no task depends on a later one (task.x = type | replica << 2).
-void cholesky_batch_tasks(const std::vector<int>& nt_of_replica, std::vector<int4>& tasks);
+// One replica's task list (task.x = type, replica tag 0) cut into segments
+// that a batch interleaves with the other replicas' (see cholesky_df.cu);
+// task.x = type | replica << 2 in the merged list.
+void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start);
 // ctl: 4 ints (next task, abort, spin failures, error bits), zero before the launch.
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
                           cudaStream_t st);

@@ -152,6 +152,7 @@ class Server:
         active = {}  # slot -> [request, steps left, bytes]
         used = 0
         peak_used, peak_active, batched_steps = 0, 0, 0
+        t_step = t_admin = 0.0
         start = time.perf_counter()
         vnow = 0.0
 
@@ -167,8 +168,10 @@ class Server:
                 if used + fp > self.memory_budget or (self.max_active and len(active) >= self.max_active):
                     break
                 pending.popleft()
+                t0 = time.perf_counter()
                 slot = self.batch.add(r.positions, r.radii, r.box_length, T=r.T, viscosity=r.viscosity,
                                       seed=r.seed, noise="device")
+                t_admin += time.perf_counter() - t0
                 active[slot] = [r, r.steps, fp]
                 used += fp
                 records[r.rid].admitted = now()
@@ -185,7 +188,9 @@ class Server:
             dts = {a[0].dt for a in active.values()}
             if len(dts) != 1:
                 raise ValueError("requests running together must share dt")
+            t0 = time.perf_counter()
             self.batch.propagate(dts.pop())
+            t_step += time.perf_counter() - t0
             batched_steps += 1
             if clock == "virtual":
                 vnow += tick
@@ -196,6 +201,7 @@ class Server:
                     done.append(slot)
             if done:
                 t_done = now()
+                t0 = time.perf_counter()
                 for slot in done:
                     r, _, fp = active.pop(slot)
                     rec = records[r.rid]
@@ -204,6 +210,7 @@ class Server:
                         rec.positions = self.batch.positions(slot).copy()
                     self.batch.remove(slot)
                     used -= fp
+                t_admin += time.perf_counter() - t0
         elapsed = now() if clock == "virtual" else time.perf_counter() - start
         recs = [records[r.rid] for r in reqs]
         lat = np.array([x.latency for x in recs]) if recs else np.array([0.0])
@@ -216,6 +223,8 @@ class Server:
             "elapsed_s": elapsed,
             "batched_steps": batched_steps,
             "peak_active": peak_active,
+            "step_s": t_step,      # wall time inside batched steps (membership rebuilds included)
+            "admin_s": t_admin,    # wall time adding and removing replicas
             "peak_bytes": peak_used,
             "memory_budget": self.memory_budget,
         }
