@@ -18,7 +18,9 @@
 // depend on which other replicas share the batch.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -26,6 +28,27 @@
 #include "pybrown_b200.h"
 
 namespace pbg {
+
+// The stream-ordered pool keeps freed replica memory for the next replica
+// instead of returning it to the driver at every synchronisation.
+inline void batch_pool_keep() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
 
 struct BatchReplica {
   pbg_params p;
@@ -256,12 +279,19 @@ __global__ void batch_noise_kernel(const BatchDev* __restrict__ reps, const unsi
 
 inline size_t elem_size(int precision) { return precision == PBG_PREC_FP64 ? 8 : 4; }
 
+// Replica buffers come from the stream-ordered pool on the legacy default
+// stream: allocation and release are ordered after the batch's earlier work
+// on that stream (and on every blocking stream) and need no device-wide sync.
 void free_replica(BatchReplica* r) {
   if (!r) return;
   void* bufs[] = {r->pos, r->radii, r->force, r->U, r->xi, r->D, r->B, r->invdiag, r->phase, r->tasks};
   for (void* p : bufs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, 0);
   delete r;
+}
+
+bool pool_alloc(void* p, size_t bytes) {
+  return cudaMallocAsync(static_cast<void**>(p), bytes, 0) == cudaSuccess;
 }
 
 template <typename P>
@@ -556,20 +586,19 @@ PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, 
   r->nt = r->ld / PBG_TILE;
   r->scale = p->kBT * 1e19 / p->viscosity;
   const size_t es = elem_size(b->precision), ld = r->ld;
-  bool ok = cudaMalloc(&r->pos, r->n * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&r->radii, r->N * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&r->force, ld * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&r->U, ld * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&r->xi, ld * sizeof(double)) == cudaSuccess &&
-            cudaMalloc(&r->D, ld * ld * es) == cudaSuccess && cudaMalloc(&r->B, ld * ld * es) == cudaSuccess &&
-            cudaMalloc(&r->invdiag, (size_t)r->nt * PBG_TILE * PBG_TILE * es) == cudaSuccess;
+  batch_pool_keep();
+  bool ok = pool_alloc(&r->pos, r->n * sizeof(double)) && pool_alloc(&r->radii, r->N * sizeof(double)) &&
+            pool_alloc(&r->force, ld * sizeof(double)) && pool_alloc(&r->U, ld * sizeof(double)) &&
+            pool_alloc(&r->xi, ld * sizeof(double)) && pool_alloc(&r->D, ld * ld * es) &&
+            pool_alloc(&r->B, ld * ld * es) && pool_alloc(&r->invdiag, (size_t)r->nt * PBG_TILE * PBG_TILE * es);
   const size_t ph = phase_scratch_bytes(r->N, b->tables, b->precision);
-  if (ok && ph) ok = cudaMalloc(&r->phase, ph) == cudaSuccess;
+  if (ok && ph) ok = pool_alloc(&r->phase, ph);
   std::vector<int4> tasks;
   cholesky_replica_tasks(r->nt, tasks, r->seg_start);
   if (ok && !tasks.empty()) {
-    ok = cudaMalloc(&r->tasks, tasks.size() * sizeof(int4)) == cudaSuccess &&
-         cudaMemcpy(r->tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = pool_alloc(&r->tasks, tasks.size() * sizeof(int4)) &&
+         cudaMemcpyAsync(r->tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, 0) ==
+             cudaSuccess;
   }
   if (!ok) {
     cudaGetLastError();
@@ -577,11 +606,13 @@ PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, 
     pbg_set_error_message("out of device memory adding a replica of %d beads", p->n_beads);
     return PBG_ERR_NOMEM;
   }
-  cudaMemset(r->force, 0, ld * sizeof(double));
-  cudaMemset(r->U, 0, ld * sizeof(double));
-  cudaMemset(r->xi, 0, ld * sizeof(double));
-  PBG_CUDA_TRY(cudaMemcpy(r->pos, pos, r->n * sizeof(double), cudaMemcpyDefault));
-  PBG_CUDA_TRY(cudaMemcpy(r->radii, radii, r->N * sizeof(double), cudaMemcpyDefault));
+  cudaMemsetAsync(r->force, 0, ld * sizeof(double), 0);
+  cudaMemsetAsync(r->U, 0, ld * sizeof(double), 0);
+  cudaMemsetAsync(r->xi, 0, ld * sizeof(double), 0);
+  // ordered on the legacy stream after the allocations; a pageable source is
+  // staged before the call returns
+  PBG_CUDA_TRY(cudaMemcpyAsync(r->pos, pos, r->n * sizeof(double), cudaMemcpyDefault, 0));
+  PBG_CUDA_TRY(cudaMemcpyAsync(r->radii, radii, r->N * sizeof(double), cudaMemcpyDefault, 0));
   int s = 0;
   while (s < (int)b->slots.size() && b->slots[s]) ++s;
   if (s == (int)b->slots.size()) b->slots.push_back(nullptr);
@@ -603,7 +634,6 @@ PBG_API int pbg_batch_remove(pbg_batch* b, int slot) {
     pbg_set_error_message("pbg_batch_remove inside a step");
     return PBG_ERR_STATE;
   }
-  PBG_CUDA_TRY(cudaDeviceSynchronize());
   free_replica(r);
   b->slots[slot] = nullptr;
   b->dirty = true;
