@@ -415,7 +415,7 @@ def run_serve_section(args, torch):
     recs, summary = server.run(stream, clock="wall")
     server.batch.close()
     summary["workload"] = (f"Poisson 50 req/s for {args.serve_seconds:g} s, N log-U[16,2048], a~U[10,40], "
-                           f"phi=0.05, steps U[{lo},{hi}] (full stream: 60 s, steps U[100,5000], about 40x "
+                           f"phi=0.05, steps U[{lo},{hi}] (full stream: 60 s, steps U[100,5000], about 150x "
                            f"the work per request), dt=1, mixed, device noise")
     summary["offered_bead_steps_per_s"] = sum(r.n_beads * r.steps for r in stream) / args.serve_seconds
     summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
