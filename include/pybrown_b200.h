@@ -203,6 +203,11 @@ PBG_API int pbg_destroy(pbg_system *sys);
 PBG_API int pbg_set_state(pbg_system *sys, const double *pos, const double *radii, const int *conn,
                   void *stream);
 PBG_API int pbg_set_force(pbg_system *sys, const double *force, void *stream);
+/* Divergence term of the lubricated diffusion matrix (box.py:211-215,
+ * 560-610; JSON "divergence_term"): in the rpy_lub / rpy_smith_lub modes with
+ * the Ermak scheme, pbg_step_begin adds div(D) dt after the deterministic
+ * step, div(D) by forward differences (eps = 1e-7, 3N rebuilds of D). */
+PBG_API int pbg_set_divergence(pbg_system *sys, int on);
 PBG_API int pbg_get_positions(pbg_system *sys, double *pos_out, void *stream);
 /* Copy matrix `which` (PBG_MAT_*) as a dense row-major 3N x 3N FP64 array
  * (host or device memory; host output synchronises the stream). */

@@ -202,6 +202,7 @@ class OracleBox:
         return self.c.overlaps(self.pos, self.radii, self.L, self.thr)
 
     def propagate(self, dt, build_Dff=True, build_Dnf=True, cholesky=True):
+        self._b_ff, self._b_nf = build_Dff, build_Dnf
         self._build(build_Dff, build_Dnf, cholesky)
         if self.scheme == "ermak":
             self._ermak(dt)
@@ -215,9 +216,30 @@ class OracleBox:
                 while self.pos[i, k] >= self.L / 2:
                     self.pos[i, k] -= self.L
 
+    # box.py:560-610: forward-difference divergence of D, eps = 1e-7.  Each
+    # coordinate is moved by +eps and back by -eps (not restored from a copy),
+    # as the reference's bead.translate does; the matrices are restored.
+    def _divergence(self, b_ff, b_nf):
+        eps = 0.0000001
+        saved = (self.D.copy(), self.Mff.copy(), self.Rff.copy(), self.R.copy())
+        div = -np.sum(self.D, axis=1)
+        for i in range(self.pos.shape[0]):
+            for j in range(3):
+                self.pos[i, j] += eps
+                if b_ff:
+                    self._dff()
+                if b_nf:
+                    self._dtot()
+                div += self.D[3 * i + j]
+                self.pos[i, j] += -eps
+        self.D, self.Mff, self.Rff, self.R = saved
+        return div / eps
+
     # box.py:202-250
     def _ermak(self, dt):
         self._det(dt)
+        if self.inp.get("divergence_term") and self.hydro in ("rpy_lub", "rpy_smith_lub"):
+            self._translate(self._divergence(self._b_ff, self._b_nf) * dt)
         count = 0
         while True:
             count += 1

@@ -96,6 +96,7 @@ _SIGNATURES = {
     "pbg_destroy": (_i, [_vp]),
     "pbg_set_state": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "pbg_set_force": (_i, [_vp, _vp, _vp]),
+    "pbg_set_divergence": (_i, [_vp, _i]),
     "pbg_get_positions": (_i, [_vp, _vp, _vp]),
     "pbg_get_matrix": (_i, [_vp, _i, _vp, _vp]),
     "pbg_set_matrix": (_i, [_vp, _i, _vp, _vp]),

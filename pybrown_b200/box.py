@@ -159,6 +159,10 @@ class Box:
         params = self._params()
         _lib.call("pbg_create", _lib.ctypes.byref(params), _lib.ctypes.byref(handle))
         self._h = handle
+        if self.inp.get("divergence_term"):
+            # box.py:211-215: only the lubrication modes under Ermak use it;
+            # the library ignores it elsewhere, as the reference does.
+            _lib.call("pbg_set_divergence", self._h, 1)
         N = len(self.beads)
         self._pos = np.ascontiguousarray(np.array([b.r for b in self.beads], dtype=np.float64).reshape(N, 3))
         for i, b in enumerate(self.beads):

@@ -330,6 +330,11 @@ int pbg_set_state(pbg_system* sys, const double* pos, const double* radii, const
   return pbg::system_set_state(sys, pos, radii, conn, (cudaStream_t)stream);
 }
 
+int pbg_set_divergence(pbg_system* sys, int on) {
+  if (!sys) return PBG_ERR_ARG;
+  return pbg::set_divergence(sys, on != 0);
+}
+
 int pbg_set_force(pbg_system* sys, const double* force, void* stream) {
   if (!sys) return PBG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;

@@ -93,7 +93,7 @@ void destroy_system(pbg_system* s) {
   void* ptrs[] = {s->pos,  s->pos_snap, s->radii, s->conn,  s->force, s->D,     s->B,    s->D0,
                   s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
                   s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
-                  s->chol_work, s->inv_work, s->dflags};
+                  s->chol_work, s->inv_work, s->dflags, s->div};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
@@ -310,6 +310,87 @@ static int stochastic_step(pbg_system* s, double mult, cudaStream_t st) {
   return launch_translate(s->pos, s->BX, s->n, false, st);
 }
 
+// ---- divergence of the lubricated D (box.py:560-610) ----------------------
+__global__ void neg_rowsum_kernel(const double* __restrict__ D, int n, int ld, double* __restrict__ out) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int c = lane; c < n; c += 32) s += D[(size_t)row * ld + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[row] = -s;
+}
+
+__global__ void add_row_kernel(const double* __restrict__ D, int m, int n, int ld, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] += D[(size_t)m * ld + k];
+}
+
+__global__ void add_scalar_kernel(double* p, int idx, double v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) p[idx] = p[idx] + v;
+}
+
+__global__ void div_apply_kernel(double* __restrict__ div, int n, double eps, double dt, double* __restrict__ pos) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double d = div[k] / eps;
+  div[k] = d;
+  pos[k] += d * dt;
+}
+
+int set_divergence(pbg_system* s, bool on) {
+  if (on && !s->div) {
+    const size_t mat = (size_t)s->ld * s->ld;
+    bool ok = cudaMalloc(&s->div, s->ld * sizeof(double)) == cudaSuccess;
+    if (ok && !s->D0) ok = cudaMalloc(&s->D0, mat * s->es) == cudaSuccess;
+    if (ok && s->lub && !s->Mff0) ok = cudaMalloc(&s->Mff0, mat * sizeof(double)) == cudaSuccess;
+    if (ok && s->lub && !s->Rff0) ok = cudaMalloc(&s->Rff0, mat * sizeof(double)) == cudaSuccess;
+    if (ok && s->lub && !s->R0) ok = cudaMalloc(&s->R0, mat * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      pbg_set_error_message("out of device memory for the divergence term");
+      return PBG_ERR_NOMEM;
+    }
+  }
+  s->divergence = on;
+  return PBG_OK;
+}
+
+// After the deterministic step of the Ermak scheme in the lubrication modes
+// (box.py:211-215): div = (sum over coordinates m of row m of D at the
+// position moved by eps in m, minus the row sums of D) / eps, by forward
+// differences with eps = 1e-7 (box.py:560-610), then pos += div dt.  The
+// matrices of the step are restored afterwards.
+static int divergence_step(pbg_system* s, cudaStream_t st) {
+  const double eps = 0.0000001;
+  const int n = s->n, ld = s->ld;
+  const size_t bytes = (size_t)ld * ld * s->es, bytes64 = (size_t)ld * ld * sizeof(double);
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->D0, s->D, bytes, cudaMemcpyDeviceToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->Mff0, s->Mff, bytes64, cudaMemcpyDeviceToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->Rff0, s->Rff, bytes64, cudaMemcpyDeviceToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->R0, s->R, bytes64, cudaMemcpyDeviceToDevice, st));
+  neg_rowsum_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>((const double*)s->D, n, ld, s->div);
+  PBG_CHECK_LAUNCH();
+  int rc;
+  for (int m = 0; m < n; ++m) {
+    add_scalar_kernel<<<1, 32, 0, st>>>(s->pos, m, eps);
+    PBG_CHECK_LAUNCH();
+    if (s->build_Dff && (rc = compute_Dff(s, st))) return rc;
+    if (s->build_Dnf && (rc = compute_Dtot(s, st))) return rc;
+    add_row_kernel<<<(n + 255) / 256, 256, 0, st>>>((const double*)s->D, m, n, ld, s->div);
+    PBG_CHECK_LAUNCH();
+    add_scalar_kernel<<<1, 32, 0, st>>>(s->pos, m, -eps);
+    PBG_CHECK_LAUNCH();
+  }
+  std::swap(s->D, s->D0);
+  std::swap(s->Mff, s->Mff0);
+  std::swap(s->Rff, s->Rff0);
+  std::swap(s->R, s->R0);
+  div_apply_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->div, n, eps, s->dt, s->pos);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
 int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st) {
   if (!s->have_state) {
     pbg_set_error_message("pbg_step_begin before pbg_set_state");
@@ -328,6 +409,8 @@ int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol,
   }
   const double mult = s->p.propagation_scheme == PBG_SCHEME_MIDPOINT ? 1.0 / s->p.m_midpoint : 1.0;
   if ((rc = deterministic_step(s, s->D, mult, st))) return rc;
+  if (s->divergence && s->lub && s->p.propagation_scheme == PBG_SCHEME_ERMAK && (rc = divergence_step(s, st)))
+    return rc;
   s->in_step = true;
   return PBG_OK;
 }

@@ -30,6 +30,8 @@ struct pbg_system {
   void* chol_work = nullptr;   // inverted diagonal tiles of B
   void* inv_work = nullptr;    // SPD inverse workspace
   int* dflags = nullptr;       // [0] overlap, [1] cholesky info, [2] Rff info, [3] D info
+  bool divergence = false;     // divergence term of the lubricated D (Ermak scheme)
+  double* div = nullptr;       // ld: its value this step
   int* hflags = nullptr;       // pinned mirror
 
   bool have_state = false;
@@ -49,6 +51,7 @@ int compute_Dff(pbg_system* s, cudaStream_t st);
 int compute_Dtot(pbg_system* s, cudaStream_t st);
 int decompose(pbg_system* s, cudaStream_t st);
 int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st);
+int set_divergence(pbg_system* s, bool on);
 int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st);
 int step_end(pbg_system* s, cudaStream_t st);
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
