@@ -203,11 +203,65 @@ PBG_API int pbg_destroy(pbg_system *sys);
 PBG_API int pbg_set_state(pbg_system *sys, const double *pos, const double *radii, const int *conn,
                   void *stream);
 PBG_API int pbg_set_force(pbg_system *sys, const double *force, void *stream);
+/* Replaces the positions only (N*3, host or device), keeping radii and bonds. */
+PBG_API int pbg_set_positions(pbg_system *sys, const double *pos, void *stream);
 /* Divergence term of the lubricated diffusion matrix (box.py:211-215,
  * 560-610; JSON "divergence_term"): in the rpy_lub / rpy_smith_lub modes with
  * the Ermak scheme, pbg_step_begin adds div(D) dt after the deterministic
  * step, div(D) by forward differences (eps = 1e-7, 3N rebuilds of D). */
 PBG_API int pbg_set_divergence(pbg_system *sys, int on);
+
+/* Immobile beads (box.py:649-668; JSON "immobile_labels").  The system's
+ * n_beads are the mobile beads; D, B and the noise cover them only, as in the
+ * reference.  Immobile beads enter the overlap test (bead.c:169-218 over all
+ * beads) and the inter-bead forces.  Host or device pointers:
+ *   pos, radii   n_immobile x 3 and n_immobile doubles;
+ *   order        n_beads + n_immobile ints: each bead's index in the caller's
+ *                full bead list, mobile beads first (NULL: mobile beads come
+ *                first in that list); it fixes the sign convention of the
+ *                overlap test's pair vectors, as bead.c:180-182 does;
+ *   conn_mi      n_beads x n_immobile int32 bond flags (NULL: none).
+ * Call again to replace; n_immobile = 0 removes them. */
+PBG_API int pbg_set_immobile(pbg_system *sys, int n_immobile, const double *pos, const double *radii,
+                             const int *order, const int *conn_mi, void *stream);
+
+/* Inter-bead forces on the device (interactions.py:483-821): Lennard-Jones
+ * between all bead pairs, harmonic bonds and harmonic angles.  Bead indices
+ * are combined: 0..n_beads-1 the mobile beads, n_beads.. the immobile ones.
+ * Each bond and angle term appears once, in the order the reference's loops
+ * meet it (interactions.py:185-247, 291-414), with the pair-vector form those
+ * loops use.  The force of a step is the pbg_set_force vector plus
+ * unit_scale times these terms, evaluated at the step-start positions by
+ * pbg_step_begin; the energy (interaction units, like the reference's Box.E)
+ * is read with pbg_get_energy.  Arrays may be host or device memory. */
+#define PBG_LJ_NONE 0
+#define PBG_LJ_6 6      /* LJ_6_attractive (interactions.py:711-745) */
+#define PBG_LJ_12 12    /* LJ_12_repulsive (interactions.py:747-781) */
+#define PBG_LJ_6_12 612 /* LJ_6_12 (interactions.py:783-821) */
+/* Pair-vector forms of an angle term (interactions.py:291-414); P(a,b) is
+ * the minimum-image vector from bead a to bead b. */
+#define PBG_ANGLE_DIRECT 0    /* p12 = P(i,j), p23 = P(j,k) */
+#define PBG_ANGLE_P23_DIFF 1  /* p23 = P(i,k) - P(i,j)  (j, k immobile) */
+#define PBG_ANGLE_P12_DIFF 2  /* p12 = P(i,k) - P(j,k)  (i, j immobile) */
+typedef struct pbg_interactions {
+  int lennard_jones;               /* PBG_LJ_* */
+  double lennard_jones_alpha;
+  const double *hard_core_radius;  /* n_beads + n_immobile */
+  const double *epsilon_lj;        /* n_beads + n_immobile */
+  int n_bonds;
+  const int *bonds;                /* 2 per bond: a, b; F_a += f, F_b -= f (mobile ends) */
+  const double *bond_params;       /* 2 per bond: dist_eq [A], force_constant */
+  int n_angles;
+  const int *angles;               /* 4 per angle: i, j, k, PBG_ANGLE_* form */
+  const double *angle_params;      /* 2 per angle: angle_eq [deg], force_constant */
+  double unit_scale;               /* 1 (joule), 6.9477e-21 (kcal/mol), 1.602176634e-19 (eV) */
+} pbg_interactions;
+/* NULL removes the interactions. */
+PBG_API int pbg_set_interactions(pbg_system *sys, const pbg_interactions *desc);
+/* Interaction energy at the start of the last step (0 without interactions). */
+PBG_API int pbg_get_energy(pbg_system *sys, double *energy_host, void *stream);
+/* Force vector (3N, joules) used by the last step. */
+PBG_API int pbg_get_force(pbg_system *sys, double *force_host, void *stream);
 PBG_API int pbg_get_positions(pbg_system *sys, double *pos_out, void *stream);
 /* Copy matrix `which` (PBG_MAT_*) as a dense row-major 3N x 3N FP64 array
  * (host or device memory; host output synchronises the stream). */

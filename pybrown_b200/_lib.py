@@ -58,6 +58,26 @@ class PbgStepReport(ctypes.Structure):
     ]
 
 
+LJ = {(False, False): 0, (True, False): 6, (False, True): 12, (True, True): 612}
+ANGLE_DIRECT, ANGLE_P23_DIFF, ANGLE_P12_DIFF = 0, 1, 2
+
+
+class PbgInteractions(ctypes.Structure):
+    _fields_ = [
+        ("lennard_jones", ctypes.c_int),
+        ("lennard_jones_alpha", ctypes.c_double),
+        ("hard_core_radius", ctypes.c_void_p),
+        ("epsilon_lj", ctypes.c_void_p),
+        ("n_bonds", ctypes.c_int),
+        ("bonds", ctypes.c_void_p),
+        ("bond_params", ctypes.c_void_p),
+        ("n_angles", ctypes.c_int),
+        ("angles", ctypes.c_void_p),
+        ("angle_params", ctypes.c_void_p),
+        ("unit_scale", ctypes.c_double),
+    ]
+
+
 class PbgError(RuntimeError):
     def __init__(self, fn, code, message):
         self.code = code
@@ -97,6 +117,11 @@ _SIGNATURES = {
     "pbg_set_state": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "pbg_set_force": (_i, [_vp, _vp, _vp]),
     "pbg_set_divergence": (_i, [_vp, _i]),
+    "pbg_set_immobile": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "pbg_set_positions": (_i, [_vp, _vp, _vp]),
+    "pbg_set_interactions": (_i, [_vp, ctypes.POINTER(PbgInteractions)]),
+    "pbg_get_energy": (_i, [_vp, _dp, _vp]),
+    "pbg_get_force": (_i, [_vp, _vp, _vp]),
     "pbg_get_positions": (_i, [_vp, _vp, _vp]),
     "pbg_get_matrix": (_i, [_vp, _i, _vp, _vp]),
     "pbg_set_matrix": (_i, [_vp, _i, _vp, _vp]),

@@ -8,36 +8,39 @@ the RPY / Smith-Ewald tensor, the Jeffrey-Onishi lubrication correction, the
 SPD inverses, the Cholesky factor, the matrix-vector products, the overlap
 test and the wrap into the box.
 
+The inter-bead forces of the reference (Lennard-Jones, harmonic bonds and
+angles, interactions.py) are evaluated on the device at the start of each
+step; immobile beads (immobile_labels) stay fixed and take part in the
+overlap test and the forces, while D, B and the noise cover the mobile beads
+only, as in the reference.
+
 The host keeps what the reference keeps on the host: the RandomState noise
 stream (drawn 3N at a time in the reference's order, box.py:393-399), the
-accept/reject loop over move attempts, and the Bead objects.  Bead.r arrays
-are views into one (N, 3) array that is refreshed from the device after each
-step, so `box.beads` always shows current positions.  Modify bead positions
-in place (Bead.translate does) or call `sync_positions_from_beads()`.
+accept/reject loop over move attempts, the Bead objects and custom
+interactions (user Python code, evaluated with the reference's loops and
+added to the external force).  The mobile beads' Bead.r arrays are views into
+one (N, 3) array that is refreshed from the device after each step, so
+`box.beads` always shows current positions.  Modify bead positions in place
+(Bead.translate does) or call `sync_positions_from_beads()`.
 
 Keywords beyond the reference's: "precision": "fp64" (default) or "mixed"
 (FP32 Ewald tensor and Cholesky trailing updates, FP64 diagonal tiles and
 position accumulation).
 """
+import ctypes
 import math
 
 import numpy as np
 from scipy.constants import Boltzmann
 
 from . import _lib
-from .bead import build_connection_matrix, check_overlaps, compute_pointer_pbc_matrix
+from .bead import (build_connection_matrix, check_overlaps, compute_pointer_immobile_pbc_matrix,
+                   compute_pointer_pbc_matrix)
+from .interactions import DeviceInteractions, eV_to_joule, kcal_per_mole_to_joule, set_custom_interactions, to_joule
+
+__all__ = ["Box", "eV_to_joule", "kcal_per_mole_to_joule"]
 
 _OUT_OF_SCOPE = ("walls", "measure_flux", "measure_concentration", "external_force_region")
-
-
-def kcal_per_mole_to_joule(value):
-    """interactions.py:823-825."""
-    return 10 ** (-21) * 6.9477 * value
-
-
-def eV_to_joule(value):
-    """interactions.py:835-837."""
-    return 10 ** (-19) * 1.602176634 * value
 
 
 class Box:
@@ -72,14 +75,16 @@ class Box:
         for key in _OUT_OF_SCOPE:
             if key in self.inp:
                 raise NotImplementedError("keyword {!r} is outside the accelerated hot path".format(key))
-        if self.inp.get("lennard_jones_6") or self.inp.get("lennard_jones_12") or \
-                self.inp.get("custom_interactions") or any(b.bonded_with or b.angled_with for b in beads):
-            raise NotImplementedError("inter-bead forces are outside the accelerated hot path")
-        self.interactions = []
+        # box.py:731-733 (interactions.py:483-515): built-in terms on the device,
+        # custom ones on the host.
+        self.custom_interactions = set_custom_interactions(self.inp)
+        self.interactions = list(self.custom_interactions)
+        self._device_interactions = DeviceInteractions(self.inp, self.mobile_beads, self.immobile_beads)
         self.reactions = []
         self.end_simulation = False
         self.is_energy = "enr_write_freq" in self.inp
         self.is_flux = self.is_concentration = self.is_wall = False
+        self._h = None
         self.E = 0.0
 
         self.overlaps = self.inp["check_overlaps"]
@@ -112,7 +117,7 @@ class Box:
         self.viscosity = self.inp["viscosity"]
 
     def _handle_bead_mobility(self):
-        """box.py:649-668 (immobile beads are outside the accelerated path)."""
+        """box.py:649-668."""
         self.immobile_labels = self.inp["immobile_labels"]
         for bead in self.beads:
             if bead.label in self.immobile_labels:
@@ -121,8 +126,6 @@ class Box:
         self.immobile_beads = [b for b in self.beads if not b.mobile]
         self.mobile_bead_indices = [i for i, b in enumerate(self.beads) if b.mobile]
         self.immobile_bead_indices = [i for i, b in enumerate(self.beads) if not b.mobile]
-        if self.immobile_beads:
-            raise NotImplementedError("immobile beads are outside the accelerated hot path")
 
     def _handle_bead_labels(self):
         self.labels = []
@@ -135,7 +138,7 @@ class Box:
 
     def _params(self):
         p = _lib.PbgParams()
-        p.n_beads = len(self.beads)
+        p.n_beads = len(self.mobile_beads)
         p.hydrodynamics = _lib.HI[self.hydrodynamics]
         p.precision = _lib.PREC[self.precision]
         p.propagation_scheme = _lib.SCHEME[self.propagation_scheme]
@@ -155,6 +158,16 @@ class Box:
 
     def _create_device_state(self, matrices=None):
         self._stream = None  # legacy default stream
+        self._h = None
+        self._device_force = None
+        mob = self.mobile_beads
+        N = len(mob)
+        self._pos = np.ascontiguousarray(np.array([b.r for b in mob], dtype=np.float64).reshape(N, 3))
+        for i, b in enumerate(mob):
+            b.r = self._pos[i]
+        self._radii = np.ascontiguousarray([b.a for b in mob], dtype=np.float64)
+        if N == 0:
+            return  # box.py:176: nothing moves
         handle = _lib.ctypes.c_void_p()
         params = self._params()
         _lib.call("pbg_create", _lib.ctypes.byref(params), _lib.ctypes.byref(handle))
@@ -163,15 +176,21 @@ class Box:
             # box.py:211-215: only the lubrication modes under Ermak use it;
             # the library ignores it elsewhere, as the reference does.
             _lib.call("pbg_set_divergence", self._h, 1)
-        N = len(self.beads)
-        self._pos = np.ascontiguousarray(np.array([b.r for b in self.beads], dtype=np.float64).reshape(N, 3))
-        for i, b in enumerate(self.beads):
-            b.r = self._pos[i]
-        self._radii = np.ascontiguousarray([b.a for b in self.beads], dtype=np.float64)
-        self._conn = np.ascontiguousarray(self.connection_matrix, dtype=np.int32) if self._has_bonds else None
+        conn = np.asarray(self.connection_matrix, dtype=np.int32)
+        mi, ii = self.mobile_bead_indices, self.immobile_bead_indices
+        conn_mm = conn[np.ix_(mi, mi)]
+        self._conn = np.ascontiguousarray(conn_mm) if conn_mm.any() else None
         _lib.call("pbg_set_state", self._h, self._pos.ctypes.data, self._radii.ctypes.data,
                   self._conn.ctypes.data if self._conn is not None else None, self._stream)
-        self._device_force = None
+        if ii:
+            pos_imm = np.ascontiguousarray([b.r for b in self.immobile_beads], dtype=np.float64).reshape(-1)
+            radii_imm = np.ascontiguousarray([b.a for b in self.immobile_beads], dtype=np.float64)
+            order = np.ascontiguousarray(mi + ii, dtype=np.int32)
+            conn_mi = np.ascontiguousarray(conn[np.ix_(mi, ii)])
+            _lib.call("pbg_set_immobile", self._h, len(ii), pos_imm.ctypes.data, radii_imm.ctypes.data,
+                      order.ctypes.data, conn_mi.ctypes.data if conn_mi.any() else None, self._stream)
+        if self._device_interactions.active:
+            self._device_interactions.install(self._h)
         if matrices:
             for name, arr in matrices.items():
                 arr = np.ascontiguousarray(arr, dtype=np.float64)
@@ -190,6 +209,8 @@ class Box:
 
     def propagate(self, dt, build_Dff=True, build_Dnf=True, cholesky=True):
         """One step (box.py:150-198) on the GPU."""
+        if self._h is None:
+            return
         self._upload_positions()
         self._compute_forces()
         h, st = self._h, self._stream
@@ -221,14 +242,21 @@ class Box:
         self.F = np.array(list(self.Fex) * (len(self.mobile_beads)))
 
     def _compute_forces(self):
-        """box.py:404-428 (external force only)."""
+        """box.py:404-428.  The external force and the custom interactions are
+        summed here; pbg_step_begin adds the built-in interactions."""
         self.E = 0.0
         self._prepare_external_force()
-        if self.inp["energy_unit"] == "kcal/mol":
-            self.F = kcal_per_mole_to_joule(self.F)
-        elif self.inp["energy_unit"] == "eV":
-            self.F = eV_to_joule(self.F)
-        F = np.ascontiguousarray(self.F, dtype=np.float64)
+        if self.custom_interactions:
+            rij = compute_pointer_pbc_matrix(self.mobile_beads, self.box_length)
+            rik = (compute_pointer_immobile_pbc_matrix(self.mobile_beads, self.immobile_beads, self.box_length)
+                   if self.immobile_beads else [])
+            F = self._F
+            for interaction in self.custom_interactions:
+                self._E_host += interaction.compute_forces_and_energy(
+                    mobile_beads=self.mobile_beads, pointers_mobile=rij, F=F,
+                    immobile_beads=self.immobile_beads, pointers_mobile_immobile=rik)
+        self.F = to_joule(self._F, self.inp["energy_unit"])
+        F = np.ascontiguousarray(self._F, dtype=np.float64)
         if self._device_force is None or not np.array_equal(F, self._device_force):
             _lib.call("pbg_set_force", self._h, F.ctypes.data, self._stream)
             self._device_force = F.copy()
@@ -237,12 +265,17 @@ class Box:
         return check_overlaps(self.beads, self.box_length, self.inp["overlap_treshold"], self.connection_matrix)
 
     def _upload_positions(self):
-        _lib.call("pbg_set_state", self._h, self._pos.ctypes.data, self._radii.ctypes.data,
-                  self._conn.ctypes.data if self._conn is not None else None, self._stream)
+        radii = [b.a for b in self.mobile_beads]
+        if not np.array_equal(radii, self._radii):
+            self._radii = np.ascontiguousarray(radii, dtype=np.float64)
+            _lib.call("pbg_set_state", self._h, self._pos.ctypes.data, self._radii.ctypes.data,
+                      self._conn.ctypes.data if self._conn is not None else None, self._stream)
+        else:
+            _lib.call("pbg_set_positions", self._h, self._pos.ctypes.data, self._stream)
 
     def sync_positions_from_beads(self):
         """Re-link Bead.r to the box after a caller replaced a bead's r array."""
-        for i, b in enumerate(self.beads):
+        for i, b in enumerate(self.mobile_beads):
             if b.r is not self._pos[i] and not (b.r.base is self._pos):
                 self._pos[i] = b.r
                 b.r = self._pos[i]
@@ -254,10 +287,37 @@ class Box:
     # ------------------------------------------------------------------ views
 
     def _matrix(self, name):
-        n = 3 * len(self.beads)
+        n = 3 * len(self.mobile_beads)
         out = np.empty((n, n), dtype=np.float64)
         _lib.call("pbg_get_matrix", self._h, _lib.MAT[name], out.ctypes.data, self._stream)
         return out
+
+    @property
+    def E(self):
+        """Interaction energy at the start of the last step (box.py:406-412)."""
+        e = self._E_host
+        if self._h is not None and self._device_interactions.active:
+            v = ctypes.c_double(0.0)
+            _lib.call("pbg_get_energy", self._h, ctypes.byref(v), self._stream)
+            e += v.value
+        return e
+
+    @E.setter
+    def E(self, value):
+        self._E_host = value
+
+    @property
+    def F(self):
+        """Force vector of the last step in joules (box.py:404-428)."""
+        if self._h is not None and self._device_interactions.active:
+            out = np.empty(3 * len(self.mobile_beads), dtype=np.float64)
+            _lib.call("pbg_get_force", self._h, out.ctypes.data, self._stream)
+            return out
+        return self._F
+
+    @F.setter
+    def F(self, value):
+        self._F = value
 
     @property
     def D(self):
@@ -287,7 +347,9 @@ class Box:
 
     def __getstate__(self):
         """Restart files (output.py:72-84) carry the device state as host arrays."""
-        state = {k: v for k, v in self.__dict__.items() if k not in ("_h", "_stream", "_pos", "_device_force")}
+        state = {k: v for k, v in self.__dict__.items()
+                 if k not in ("_h", "_stream", "_pos", "_device_force", "_device_interactions",
+                              "custom_interactions", "interactions")}
         mats = {"D": self.D, "B": self.B}
         if self.hydrodynamics in ("rpy_lub", "rpy_smith_lub"):
             mats.update(Mff=self.Mff, Rff=self.Rff, R=self.R)
@@ -297,6 +359,9 @@ class Box:
     def __setstate__(self, state):
         mats = state.pop("_device_matrices", None)
         self.__dict__.update(state)
+        self.custom_interactions = set_custom_interactions(self.inp)
+        self.interactions = list(self.custom_interactions)
+        self._device_interactions = DeviceInteractions(self.inp, self.mobile_beads, self.immobile_beads)
         self._create_device_state(matrices=mats)
 
     def __str__(self):

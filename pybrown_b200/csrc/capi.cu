@@ -335,6 +335,47 @@ int pbg_set_divergence(pbg_system* sys, int on) {
   return pbg::set_divergence(sys, on != 0);
 }
 
+int pbg_set_positions(pbg_system* sys, const double* pos, void* stream) {
+  if (!sys || !pos) return PBG_ERR_ARG;
+  if (!sys->have_state) {
+    pbg_set_error_message("pbg_set_positions before pbg_set_state");
+    return PBG_ERR_STATE;
+  }
+  PBG_CUDA_TRY(cudaMemcpyAsync(sys->pos, pos, sys->N * 3 * sizeof(double), cudaMemcpyDefault, (cudaStream_t)stream));
+  return PBG_OK;
+}
+
+int pbg_set_immobile(pbg_system* sys, int n_immobile, const double* pos, const double* radii, const int* order,
+                     const int* conn_mi, void* stream) {
+  if (!sys) return PBG_ERR_ARG;
+  return pbg::set_immobile(sys, n_immobile, pos, radii, order, conn_mi, (cudaStream_t)stream);
+}
+
+int pbg_set_interactions(pbg_system* sys, const pbg_interactions* desc) {
+  if (!sys) return PBG_ERR_ARG;
+  return pbg::set_interactions(sys, desc);
+}
+
+int pbg_get_energy(pbg_system* sys, double* energy_host, void* stream) {
+  if (!sys || !energy_host) return PBG_ERR_ARG;
+  if (!sys->energy) {
+    *energy_host = 0.0;
+    return PBG_OK;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  PBG_CUDA_TRY(cudaMemcpyAsync(energy_host, sys->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  return PBG_OK;
+}
+
+int pbg_get_force(pbg_system* sys, double* force_host, void* stream) {
+  if (!sys || !force_host) return PBG_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  PBG_CUDA_TRY(cudaMemcpyAsync(force_host, pbg::step_force(sys), sys->n * sizeof(double), cudaMemcpyDefault, st));
+  PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  return PBG_OK;
+}
+
 int pbg_set_force(pbg_system* sys, const double* force, void* stream) {
   if (!sys) return PBG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;

@@ -90,6 +90,8 @@ static int sys_alloc(void** p, size_t bytes, F&&) {
 
 void destroy_system(pbg_system* s) {
   if (!s) return;
+  free_interactions(s);
+  free_immobile(s);
   void* ptrs[] = {s->pos,  s->pos_snap, s->radii, s->conn,  s->force, s->D,     s->B,    s->D0,
                   s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
                   s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
@@ -288,6 +290,7 @@ static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
   if (!s->p.check_overlaps) return PBG_OK;
   int rc = launch_overlap(s->pos, s->radii, s->N, s->p.box_length, s->p.overlap_treshold, s->conn, s->dflags, st);
   if (rc) return rc;
+  if ((rc = overlap_immobile(s, s->dflags, st))) return rc;
   PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   PBG_CUDA_TRY(cudaStreamSynchronize(st));
   *overlap = s->hflags[0] != 0;
@@ -296,7 +299,7 @@ static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
 
 // Deterministic step (box.py:353-362): pos += ((dt/kBT) D @ F) * mult.
 static int deterministic_step(pbg_system* s, const void* D, double mult, cudaStream_t st) {
-  int rc = launch_gemv_scaled(D, s->ld, s->n, s->prec, s->force, s->dt / s->p.kBT, s->FX, st);
+  int rc = launch_gemv_scaled(D, s->ld, s->n, s->prec, step_force(s), s->dt / s->p.kBT, s->FX, st);
   if (rc) return rc;
   rc = launch_scale2(s->FX, 1.0, mult, s->n, s->FX, st);
   if (rc) return rc;
@@ -407,6 +410,8 @@ int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol,
     if (s->lub && build_Dnf && (rc = compute_Dtot(s, st))) return rc;
     if (chol && (rc = decompose(s, st))) return rc;
   }
+  // box.py:186: forces at the step-start positions, after the matrices.
+  if ((rc = compute_forces(s, st))) return rc;
   const double mult = s->p.propagation_scheme == PBG_SCHEME_MIDPOINT ? 1.0 / s->p.m_midpoint : 1.0;
   if ((rc = deterministic_step(s, s->D, mult, st))) return rc;
   if (s->divergence && s->lub && s->p.propagation_scheme == PBG_SCHEME_ERMAK && (rc = divergence_step(s, st)))
@@ -498,7 +503,8 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
   }
   if ((rc = midpoint_rebuild(s, st))) return rc;
   // deterministic drift m dt / (2 kBT) (D' - D0) @ F
-  if ((rc = launch_gemv_diff(s->D, s->D0, s->ld, n, s->prec, s->force, m * s->dt / (2 * s->p.kBT), s->ddet, st)))
+  if ((rc = launch_gemv_diff(s->D, s->D0, s->ld, n, s->prec, step_force(s), m * s->dt / (2 * s->p.kBT), s->ddet,
+                             st)))
     return rc;
   // stochastic drift m/2 sqrt(2 dt) (D' inv(B0^T) - B0) @ xi = c2 (D' y - B0 xi), B0^T y = xi
   if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) return rc;

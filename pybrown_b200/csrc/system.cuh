@@ -6,6 +6,10 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+namespace pbg {
+struct ForceField;
+}
+
 struct pbg_system {
   pbg_params p{};
   int N = 0, n = 0, ld = 0;  // beads, matrix order 3N, padded order
@@ -34,6 +38,17 @@ struct pbg_system {
   double* div = nullptr;       // ld: its value this step
   int* hflags = nullptr;       // pinned mirror
 
+  // Immobile beads (box.py:649-668): overlap partners and force sources only.
+  int M = 0;
+  double* pos_imm = nullptr;   // M x 3
+  double* radii_imm = nullptr; // M
+  int* order = nullptr;        // N + M: index in the caller's full bead list
+  int* conn_mi = nullptr;      // N x M bond flags, or null
+  // Inter-bead forces (interactions.py); null without them.
+  pbg::ForceField* ff = nullptr;
+  double* ftot = nullptr;      // ld: force of the step (base + interactions)
+  double* energy = nullptr;    // interaction energy of the step (device scalar)
+
   bool have_state = false;
   bool in_step = false;
   double dt = 0;
@@ -56,5 +71,15 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
 int step_end(pbg_system* s, cudaStream_t st);
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
 int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st);
+int set_immobile(pbg_system* s, int M, const double* pos, const double* radii, const int* order,
+                 const int* conn_mi, cudaStream_t st);
+int set_interactions(pbg_system* s, const pbg_interactions* d);
+void free_interactions(pbg_system* s);
+void free_immobile(pbg_system* s);
+// Force of the step into s->ftot and the energy into s->energy (no-op without interactions).
+int compute_forces(pbg_system* s, cudaStream_t st);
+// Overlap of any mobile bead with any immobile one, OR-ed into *flag.
+int overlap_immobile(pbg_system* s, int* flag, cudaStream_t st);
+inline const double* step_force(const pbg_system* s) { return s->ff ? s->ftot : s->force; }
 
 }  // namespace pbg

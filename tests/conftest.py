@@ -34,6 +34,11 @@ def trajectories():
     return np.load(os.path.join(GOLDEN, "trajectories.npz"))
 
 
+@pytest.fixture(scope="session")
+def forces_golden():
+    return np.load(os.path.join(GOLDEN, "forces.npz"))
+
+
 def rel_err(a, b):
     """max |a - b| / max |b| (the matrix-level relative error used throughout)."""
     a = np.asarray(a, dtype=np.float64)
