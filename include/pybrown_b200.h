@@ -282,10 +282,15 @@ PBG_API int pbg_step_begin(pbg_system *sys, double dt, int build_Dff, int build_
 PBG_API int pbg_step_attempt(pbg_system *sys, const double *xi, int *accepted_host, void *stream);
 PBG_API int pbg_step_end(pbg_system *sys, void *stream);
 
-/* Device-resident multi-step run: steps j0 .. j0+n_steps-1 with the build
- * cadence of BD.py:177 (j % diff_freq == 0 ...).  Noise is consumed in
- * order from `pool` (device, pool_len doubles); each attempt takes 3N.
- * Never synchronises; read the outcome with pbg_run_report. */
+/* Multi-step run: steps j0 .. j0+n_steps-1 with the build cadence of
+ * BD.py:177 (j % diff_freq == 0 ...), each step as Box.propagate does it.
+ * Noise is consumed in order from `pool` (device or host, pool_len doubles);
+ * each attempt takes 3N, so a pool filled from RandomState(seed) reproduces
+ * the reference's trajectory.  The accept decision of each attempt
+ * synchronises the stream, as pbg_step_attempt does.  A step that runs out of
+ * noise (PBG_ERR_NOISE) or of move attempts (PBG_ERR_ATTEMPTS, box.py:248)
+ * is rolled back to its start positions and ends the run; pbg_run_report
+ * gives the steps completed, the noise consumed and the attempt counts. */
 PBG_API int pbg_run(pbg_system *sys, long long j0, int n_steps, double dt, int diff_freq, int lub_freq,
             int chol_freq, const double *pool, long long pool_len, void *stream);
 PBG_API int pbg_run_report(pbg_system *sys, pbg_step_report *out, void *stream);

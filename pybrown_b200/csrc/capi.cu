@@ -420,15 +420,15 @@ int pbg_step_end(pbg_system* sys, void* stream) {
 
 int pbg_run(pbg_system* sys, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
             const double* pool, long long pool_len, void* stream) {
-  (void)sys; (void)j0; (void)n_steps; (void)dt; (void)diff_freq; (void)lub_freq; (void)chol_freq;
-  (void)pool; (void)pool_len; (void)stream;
-  pbg_set_error_message("pbg_run: not available in this build");
-  return PBG_ERR_STATE;
+  if (!sys) return PBG_ERR_ARG;
+  return pbg::run(sys, j0, n_steps, dt, diff_freq, lub_freq, chol_freq, pool, pool_len, (cudaStream_t)stream);
 }
 
 int pbg_run_report(pbg_system* sys, pbg_step_report* out, void* stream) {
-  (void)sys; (void)out; (void)stream;
-  return PBG_ERR_STATE;
+  (void)stream;
+  if (!sys || !out) return PBG_ERR_ARG;
+  *out = sys->report;
+  return PBG_OK;
 }
 
 }  // extern "C"

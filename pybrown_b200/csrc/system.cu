@@ -549,6 +549,60 @@ int step_end(pbg_system* s, cudaStream_t st) {
   return PBG_OK;
 }
 
+// Steps j0 .. j0+n_steps-1 of BD.py:177 with the noise taken in order from
+// `pool`: the protocol of Box.propagate (box.py:150-250) with the pool in
+// place of RandomState.  A step that runs out of noise or of move attempts
+// (box.py:248) is rolled back to its start positions and ends the run.
+int run(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
+        const double* pool, long long pool_len, cudaStream_t st) {
+  s->report = pbg_step_report{};
+  if (n_steps < 0 || diff_freq <= 0 || lub_freq <= 0 || chol_freq <= 0 || pool_len < 0 || (!pool && n_steps > 0)) {
+    pbg_set_error_message("invalid pbg_run arguments");
+    return s->report.status = PBG_ERR_ARG;
+  }
+  if (s->in_step) {
+    pbg_set_error_message("pbg_run inside a step");
+    return s->report.status = PBG_ERR_STATE;
+  }
+  const int n = s->n;
+  const size_t pos_bytes = (size_t)s->N * 3 * sizeof(double);
+  long long used = 0;
+  int rc = PBG_OK;
+  for (int k = 0; k < n_steps; ++k) {
+    const long long j = j0 + k;
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->pos_snap, s->pos, pos_bytes, cudaMemcpyDeviceToDevice, st));
+    if ((rc = step_begin(s, dt, j % diff_freq == 0, j % lub_freq == 0, j % chol_freq == 0, st))) break;
+    int accepted = 0, attempts = 0;
+    while (!accepted) {
+      if (used + n > pool_len) {
+        pbg_set_error_message("pbg_run: the noise pool ran out in step %lld", j);
+        rc = PBG_ERR_NOISE;
+        break;
+      }
+      if ((rc = step_attempt(s, pool + used, &accepted, st))) break;
+      used += n;
+      ++attempts;
+      if (!accepted && attempts >= s->p.max_move_attempts) {
+        pbg_set_error_message("maximal number of move attempts exceeded in step %lld", j);
+        rc = PBG_ERR_ATTEMPTS;
+        break;
+      }
+    }
+    if (rc) {
+      s->in_step = false;
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->pos, s->pos_snap, pos_bytes, cudaMemcpyDeviceToDevice, st));
+      break;
+    }
+    if ((rc = step_end(s, st))) break;
+    s->report.steps_done++;
+    s->report.draws_consumed = used;
+    s->report.last_attempts = attempts;
+    s->report.max_attempts = std::max(s->report.max_attempts, attempts);
+  }
+  s->report.status = rc;
+  return rc;
+}
+
 template <typename T>
 __global__ void import_matrix_kernel(const double* __restrict__ src, int n, int ld, T* __restrict__ dst) {
   const long long total = (long long)n * n;

@@ -54,6 +54,7 @@ struct pbg_system {
   double dt = 0;
   int build_Dff = 1, build_Dnf = 1, cholesky = 1;
   int attempts = 0;
+  pbg_step_report report{};    // outcome of the last pbg_run
 };
 
 namespace pbg {
@@ -69,6 +70,8 @@ int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol,
 int set_divergence(pbg_system* s, bool on);
 int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st);
 int step_end(pbg_system* s, cudaStream_t st);
+int run(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
+        const double* pool, long long pool_len, cudaStream_t st);
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
 int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st);
 int set_immobile(pbg_system* s, int M, const double* pos, const double* radii, const int* order,
