@@ -50,7 +50,7 @@ constexpr int THREADS = 256;
 constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
-enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2 };
+enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3 };
 
 struct DFArgs {
   void* A;
@@ -108,7 +108,8 @@ __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* ta
     for (int q = 0; q < count && ok; ++q) {
       long long it = 0;
       while (ld_acquire(flags[q]) < targets[q]) {
-        if (ld_acquire(a.ctl + 1)) { ok = 0; break; }
+        // the abort flag is polled every 16th round, so a round costs one L2 trip
+        if ((it & 15) == 15 && ld_acquire(a.ctl + 1)) { ok = 0; break; }
         if (++it > a.spin_limit) {
           atomicExch(a.ctl + 1, 1);
           atomicAdd(a.ctl + 2, 1);
@@ -117,7 +118,7 @@ __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* ta
           ok = 0;
           break;
         }
-        __nanosleep(it < 64 ? 20 : 200);
+        if (it > 256) __nanosleep(200);
       }
     }
     *s_ok = ok;
@@ -325,8 +326,21 @@ __device__ __forceinline__ void load_and_update(const DFArgs& a, int i, int j, i
 // ---------------------------------------------------------------- F(k)
 template <typename T>
 __device__ __forceinline__ T rsqrt_t(T x);
+// 1/sqrt(x) for the FP64 pivots: the PTX rsqrt.approx.ftz.f64 estimate
+// refined by two Newton-Raphson steps y <- y + y (1 - x y^2) / 2, which
+// converge quadratically to full precision (measured <= 1.24 ulp over
+// [1e-30, 1e30] against a long-double reference; the library call measured
+// about 100 cycles more per pivot inside the pivot-block code).  For positive
+// normal x: subnormals are flushed to zero and x <= 0 gives inf or NaN, which
+// the factorisation reports as a non-positive pivot before it is used.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
+  return fma(0.5 * y, fma(-x * y, y, 1.0), y);
+}
 template <>
-__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
+__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt_nr(x); }
 template <>
 __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
@@ -544,6 +558,97 @@ __device__ __forceinline__ void invert_factor(const T* Lk, const T* Rinv, T* X, 
   }
 }
 
+// inv(L_kk) from Lk ([64][LDA], zero above the diagonal) and Rinv = 1 / L_jj
+// into X, then to the global invdiag array as S.  Scratch: Tm (>= 32 x 36).
+template <typename T, typename S>
+__device__ __forceinline__ void store_inverse(const DFArgs& a, int k, const T* Lk, const T* Rinv, T* X, T* Tm) {
+  invert_factor(Lk, Rinv, X, Tm);
+  S* inv = reinterpret_cast<S*>(a.invdiag) + (size_t)k * NB * NB;
+  if constexpr (sizeof(S) == sizeof(T)) {
+    store_tile(X, LDA, inv, NB);
+  } else {
+    for (int t = threadIdx.x; t < NB * NB; t += THREADS) inv[t] = (S)X[(t >> 6) * LDA + (t & 63)];
+  }
+}
+
+// The eight 8 x 8 diagonal blocks of inv(L) (L in Lk, Rinv = 1 / L_jj) into
+// XL[b][i][c] (8 x 8 x 8 doubles): warp b, lane c < 8 solves column c by
+// forward substitution.  The caller orders XL's readers after a CTA barrier.
+__device__ __forceinline__ void leaf_inverses(const double* Lk, const double* Rinv, double* XL) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane < 8) {
+    const double* D = Lk + 8 * warp * LDA + 8 * warp;
+    const double* R = Rinv + 8 * warp;
+    double x[8];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+      double sacc = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q < ii && q >= lane) sacc += D[ii * LDA + q] * x[q];
+      x[ii] = ii < lane ? 0.0 : (ii == lane ? R[ii] : -sacc * R[ii]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) XL[warp * 64 + ii * 8 + lane] = x[ii];
+  }
+}
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// C <- C inv(L)^T for the 64 x 64 tile C (T, [64][LDA] smem) by blocked
+// forward substitution in FP64 on the tensor cores: warp w owns rows
+// 8w .. 8w+7 and, for each 8-column block j,
+//   W_j = (C_j - W_{<j} L_{j,<j}^T) inv(L_jj)^T,
+// where W ([64][LDA] doubles) holds the rows in FP64 (W may alias C when T
+// is double).  L: [64][LDA] doubles, XL: leaf_inverses.  Only warp-level
+// synchronisation: every warp reads its own rows, L and XL.
+template <typename T>
+__device__ __forceinline__ void trsm_rows(const double* L, const double* XL, T* C, double* W) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = 8 * warp;
+  if constexpr (sizeof(T) != sizeof(double)) {
+    for (int e = lane; e < 8 * NB; e += 32) W[(r0 + (e >> 6)) * LDA + (e & 63)] = (double)C[(r0 + (e >> 6)) * LDA + (e & 63)];
+    __syncwarp();
+  }
+  double* Wr = W + r0 * LDA;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int c0 = 8 * j;
+    // the update's operands first, then its 2j products on four accumulators
+    double av[14], bv[14];
+    const double* Lj = L + (c0 + g) * LDA;
+#pragma unroll
+    for (int q = 0; q < 2 * j; ++q) {
+      av[q] = -Wr[g * LDA + 4 * q + t];
+      bv[q] = Lj[4 * q + t];
+    }
+    double d[4][2] = {{Wr[g * LDA + c0 + 2 * t], Wr[g * LDA + c0 + 2 * t + 1]}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int q = 0; q < 2 * j; ++q) dmma(d[q & 3], av[q], bv[q]);
+    __syncwarp();
+    Wr[g * LDA + c0 + 2 * t] = (d[0][0] + d[1][0]) + (d[2][0] + d[3][0]);
+    Wr[g * LDA + c0 + 2 * t + 1] = (d[0][1] + d[1][1]) + (d[2][1] + d[3][1]);
+    __syncwarp();
+    // times inv(L_jj)^T: B[k][n] = XL[j][n][k]
+    double e0[2] = {0.0, 0.0}, e1[2] = {0.0, 0.0};
+    const double a0 = Wr[g * LDA + c0 + t], a1 = Wr[g * LDA + c0 + 4 + t];
+    const double b0 = XL[j * 64 + g * 8 + t], b1 = XL[j * 64 + g * 8 + 4 + t];
+    dmma(e0, a0, b0);
+    dmma(e1, a1, b1);
+    __syncwarp();
+    Wr[g * LDA + c0 + 2 * t] = e0[0] + e1[0];
+    Wr[g * LDA + c0 + 2 * t + 1] = e0[1] + e1[1];
+    __syncwarp();
+  }
+  if constexpr (sizeof(T) != sizeof(double)) {
+    for (int e = lane; e < 8 * NB; e += 32) C[(r0 + (e >> 6)) * LDA + (e & 63)] = (T)W[(r0 + (e >> 6)) * LDA + (e & 63)];
+  }
+}
+
 // Factor the 64 x 64 tile held in acc (already fully updated) in T arithmetic,
 // by eight 8-column panels.  Per panel p (columns c0 = 8p .. c0+7):
 //  1. the owners copy the panel's column strip (rows >= c0) to shared memory;
@@ -560,7 +665,7 @@ __device__ __forceinline__ void invert_factor(const T* Lk, const T* Rinv, T* X, 
 // written to the global invdiag array.  Ends with a CTA barrier.
 // T is the arithmetic, S the type of the matrix in global memory (the mixed
 // path factors its FP32 diagonal tiles in FP64 and stores them rounded).
-template <typename T, typename S = T>
+template <typename T, typename S = T, bool INVERSE = true>
 __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T* fs, T* Lk, T* X) {
   constexpr int PB = Strip<T>::PB;
   T* Rinv = fs + 2 * NB * PB;  // [64] 1 / L_jj
@@ -668,13 +773,7 @@ __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T
       Lk[r * LDA + c] = v;
     }
   __syncthreads();
-  invert_factor(Lk, Rinv, X, fs);
-  S* inv = reinterpret_cast<S*>(a.invdiag) + (size_t)k * NB * NB;
-  if constexpr (sizeof(S) == sizeof(T)) {
-    store_tile(X, LDA, inv, NB);
-  } else {
-    for (int t = threadIdx.x; t < NB * NB; t += THREADS) inv[t] = (S)X[(t >> 6) * LDA + (t & 63)];
-  }
+  if constexpr (INVERSE) store_inverse<T, S>(a, k, Lk, Rinv, X, fs);
 }
 
 // F(k) of the mixed path: the FP32 tile in acc (after its last update) is
@@ -725,41 +824,44 @@ __device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
 }
 
 // Shared memory of the chain CTA: four T tiles Cp, Cn, X, sA ([64][LDA]
-// each) and the FP64 factor scratch -- in the FP64 path sA also holds L_kk
-// during F and the factor scratch follows it; in the mixed path two more
-// FP64 tiles (L_kk, inverse) come first.  Every piece is a multiple of 16
-// bytes, so each starts 16-byte aligned.
+// each) and the FP64 factor scratch -- in the FP64 path X holds L_kk from F(k)
+// to S(k+1, k); in the mixed path two more FP64 tiles (L_kk, the FP64 rows of
+// the solve) come first.  Every piece is a multiple of 16 bytes, so each
+// starts 16-byte aligned.
 template <typename T>
 constexpr size_t chain_smem_bytes() {
   return sizeof(T) * 4 * NB * LDA + (sizeof(T) == 8 ? 0 : sizeof(double) * 2 * NB * LDA) +
          sizeof(double) * factor_smem_elems<double>();
 }
 
-// The chain CTA: F(0), S(1, 0), F(1), S(2, 1), ... with L(k, k-1) and
-// inv(L_kk) kept in shared memory from one task to the next.  The last
-// update of S(k+1, k) (with panel k-1) is a worker task that runs during
-// F(k); while S(k+1, k) runs, the next diagonal tile is prefetched into shared
-// memory if its updates by the workers are already complete.
+// The chain CTA: F(0), S(1, 0), F(1), S(2, 1), ... with L(k, k-1) and the
+// FP64 L_kk kept in shared memory from one task to the next.  F(k) does not
+// form inv(L_kk) (a worker task I(k) does, for the other solves of column k);
+// S(k+1, k) is a blocked forward substitution against L_kk (trsm_rows).  The
+// last update of S(k+1, k) (with panel k-1) is a worker task that runs during
+// F(k); while S(k+1, k) runs, the next diagonal tile is prefetched into
+// shared memory if its updates by the workers are already complete.
 template <typename T>
 __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
   __shared__ int s_pf;
   T* Cp = reinterpret_cast<T*>(smem);  // L(k, k-1), the previous solve's result
   T* Cn = Cp + NB * LDA;               // this step's solve input / result L(k+1, k)
-  T* X = Cn + NB * LDA;                // inv(L_kk)
-  T* sA = X + NB * LDA;                // prefetched A_kk; L_kk at the end of F(k) (FP64 path)
-  // FP64 factor scratch: the mixed path keeps its own L_kk and inverse tiles
-  double* Lk64;
-  double* X64;
-  double* fs64;
+  T* X = Cn + NB * LDA;                // FP64 path: L_kk
+  T* sA = X + NB * LDA;                // prefetched A_kk
+  double* Lk64;  // L_kk in FP64, F(k) to S(k+1, k)
+  double* W64;   // FP64 rows of the solve (the mixed path; the FP64 path solves in Cn)
+  double* fs64;  // factor scratch; its strip area holds the leaf inverses during S
   if constexpr (sizeof(T) == 8) {
-    Lk64 = reinterpret_cast<double*>(sA);
-    X64 = reinterpret_cast<double*>(X);
+    Lk64 = reinterpret_cast<double*>(X);
+    W64 = nullptr;
     fs64 = reinterpret_cast<double*>(sA + NB * LDA);
   } else {
     Lk64 = reinterpret_cast<double*>(sA + NB * LDA);
-    X64 = Lk64 + NB * LDA;
-    fs64 = X64 + NB * LDA;
+    W64 = Lk64 + NB * LDA;
+    fs64 = W64 + NB * LDA;
   }
+  double* Rinv64 = fs64 + 2 * NB * Strip<double>::PB;
+  double* XL = fs64;
   const int nt = a.nt;
   bool pf = false;  // A_kk prefetched into sA
   for (int k = 0; k < nt; ++k) {
@@ -781,15 +883,31 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
       load_acc(tile<T>(a, 0, 0), a.ld, acc);
     }
     TRACE(1, a.ntasks + 2 * k);
-    if constexpr (sizeof(T) == 8) factor_tile<double>(a, k, acc, fs64, Lk64, X64);
-    else factor_tile_fp64(a, k, acc, fs64, Lk64, X64, X);
+    if constexpr (sizeof(T) == 8) {
+      factor_tile<double, double, false>(a, k, acc, fs64, Lk64, nullptr);
+    } else {
+      double acc64[16];
+#pragma unroll
+      for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+        for (int cs = 0; cs < 8; ++cs)
+          acc64[TileMMA<double>::idx(rs, cs)] = (double)acc[TileMMA<float>::idx(rs, cs)];
+      factor_tile<double, float, false>(a, k, acc64, fs64, Lk64, nullptr);
+    }
     publish(a.fin + k * nt + k, 1);
     TRACE(2, a.ntasks + 2 * k);
-    if (k + 1 == nt) return;
+    if (k + 1 == nt) {
+      // the last inverse has no solve task after it: form it here
+      double* X64 = sizeof(T) == 8 ? reinterpret_cast<double*>(Cn) : W64;
+      store_inverse<double, T>(a, k, Lk64, Rinv64, X64, fs64);
+      publish(a.fin + k * nt + k, 2);
+      return;
+    }
     // S(k+1, k): A(k+1,k) after updates 0 .. k-1 (other CTAs), times inv(L_kk)^T
     TRACE(0, a.ntasks + 2 * k + 1);
     TRACE(3, a.ntasks + 2 * k + 1);
     if (threadIdx.x == 0) s_pf = ld_acquire(a.upd + (k + 1) * nt + k + 1) >= k;
+    leaf_inverses(Lk64, Rinv64, XL);
     if (k > 0) {
       if (!wait_geq(a, a.upd + (k + 1) * nt + k, k, s_ok)) return;
     } else {
@@ -801,11 +919,11 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
     load_acc(tile<T>(a, k + 1, k), a.ld, acc);
     TRACE(1, a.ntasks + 2 * k + 1);
     acc_to_smem(acc, Cn);
+    __syncthreads();  // each warp solves rows that other warps stored
+    if constexpr (sizeof(T) == 8) trsm_rows<T>(Lk64, XL, Cn, reinterpret_cast<double*>(Cn));
+    else trsm_rows<T>(Lk64, XL, Cn, W64);
     __syncthreads();
-    solve_by_inverse(Cn, X, acc);
-    __syncthreads();  // every warp has read Cn
-    acc_to_smem(acc, Cn);
-    store_acc(tile<T>(a, k + 1, k), a.ld, acc);
+    store_tile(Cn, LDA, tile<T>(a, k + 1, k), a.ld);
     publish(a.fin + (k + 1) * nt + k, 1);
     TRACE(2, a.ntasks + 2 * k + 1);
     T* t = Cp;
@@ -836,7 +954,26 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
     TRACE(0, t);
     TRACE(3, t);
     T acc[16];
-    if (type == TASK_U) {
+    if (type == TASK_I) {
+      // I(k): inv(L_kk) for the solves of column k, from the stored L_kk
+      if (!wait_geq(a, a.fin + k * nt + k, 1, &s_ok)) return;
+      TRACE(1, t);
+      double* Lk = reinterpret_cast<double*>(smem);
+      double* Xw = Lk + NB * LDA;
+      double* Tm = Xw + NB * LDA;
+      double* Rv = Tm + 32 * 36;
+      const T* g = tile<T>(a, k, k);
+      for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
+        const int r = e >> 6, c = e & 63;
+        Lk[r * LDA + c] = c <= r ? (double)ldcg(g + (size_t)r * a.ld + c) : 0.0;
+      }
+      __syncthreads();
+      if (threadIdx.x < NB) Rv[threadIdx.x] = 1.0 / Lk[threadIdx.x * LDA + threadIdx.x];
+      __syncthreads();
+      store_inverse<double, T>(a, k, Lk, Rv, Xw, Tm);
+      publish(a.fin + k * nt + k, 2);
+      TRACE(2, t);
+    } else if (type == TASK_U) {
       // U(i, j, k): needs L_ik, L_jk final and the k previous updates of (i, j)
       const int* fl[3] = {a.fin + i * nt + k, a.fin + j * nt + k, a.upd + i * nt + j};
       const int tg[3] = {1, 1, k};
@@ -857,7 +994,7 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
       } else {
         load_acc(tile<T>(a, i, col), a.ld, acc);
       }
-      if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
+      if (!wait_geq(a, a.fin + col * nt + col, 2, &s_ok)) return;  // inv(L_col,col) stored
       TRACE(1, t);
       stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);
       acc_to_smem(acc, sA);
@@ -968,12 +1105,15 @@ int get_task_table(int nt, const int4** out, int* count) {
     *count = it->second.second;
     return PBG_OK;
   }
-  // The chain tasks F(k) and S(k+1, k) run on the chain CTA and are left out.
+  // The chain tasks F(k) and S(k+1, k) run on the chain CTA and are left out;
+  // so is I(nt-1), which the chain forms after its last factorisation.
   std::vector<int4> t;
+  if (nt > 1) t.push_back(make_int4(TASK_I, 0, 0, 0));
   for (int i = 2; i < nt; ++i) t.push_back(make_int4(TASK_S, i, 0, 0));
   for (int k = 0; k + 1 < nt; ++k) {
     // the last update of the chain's S(k+2, k+1), first: it runs during F(k+1)
     if (k + 2 < nt) t.push_back(make_int4(TASK_U, k + 2, k + 1, k));
+    if (k + 2 < nt) t.push_back(make_int4(TASK_I, 0, 0, k + 1));
     for (int i = k + 3; i < nt; ++i) t.push_back(make_int4(TASK_S, i, k + 1, k + 1));
     // the rest of column k+1 of the update with panel k is fused into F(k+1)
     // and the workers' S(., k+1); the plain updates cover columns >= k+2, the
