@@ -611,6 +611,7 @@ __device__ __forceinline__ void trsm_rows(const double* L, const double* XL, T* 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int r0 = 8 * warp;
   if constexpr (sizeof(T) != sizeof(double)) {
+#pragma unroll 4
     for (int e = lane; e < 8 * NB; e += 32) W[(r0 + (e >> 6)) * LDA + (e & 63)] = (double)C[(r0 + (e >> 6)) * LDA + (e & 63)];
     __syncwarp();
   }
@@ -645,6 +646,7 @@ __device__ __forceinline__ void trsm_rows(const double* L, const double* XL, T* 
     __syncwarp();
   }
   if constexpr (sizeof(T) != sizeof(double)) {
+#pragma unroll 4
     for (int e = lane; e < 8 * NB; e += 32) C[(r0 + (e >> 6)) * LDA + (e & 63)] = (T)W[(r0 + (e >> 6)) * LDA + (e & 63)];
   }
 }
@@ -665,8 +667,23 @@ __device__ __forceinline__ void trsm_rows(const double* L, const double* XL, T* 
 // written to the global invdiag array.  Ends with a CTA barrier.
 // T is the arithmetic, S the type of the matrix in global memory (the mixed
 // path factors its FP32 diagonal tiles in FP64 and stores them rounded).
+// Optional early fetch of the chain's next solve input during F(k): at the
+// start of the last panel, if *flag >= target, the tile src is staged into dst
+// ([64][LDA]) with cp.async and *ready is set (read after the tile's final
+// barrier).
+template <typename S>
+struct SolveInput {
+  const int* flag;
+  int target;
+  const S* src;
+  int ld;
+  S* dst;
+  int* ready;
+};
+
 template <typename T, typename S = T, bool INVERSE = true>
-__device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T* fs, T* Lk, T* X) {
+__device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T* fs, T* Lk, T* X,
+                                            const SolveInput<S>* pre = nullptr) {
   constexpr int PB = Strip<T>::PB;
   T* Rinv = fs + 2 * NB * PB;  // [64] 1 / L_jj
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -691,7 +708,24 @@ __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T
               if (r >= c0) P[r * PB + acc_col(cs) - c0] = acc[TileMMA<T>::idx(rs, cs)];
             }
     }
+    // warp 7 has no trailing update in the last panel: it polls the flag
+    // before the barrier, takes the value after it and stages the tile
+    int pre_v = 0;
+    if (pre && p == 7 && tid == 32 * 7) pre_v = ld_acquire(pre->flag);
     __syncthreads();
+    if (pre && p == 7 && warp == 7) {
+      const int v = __shfl_sync(0xffffffffu, pre_v, 0);
+      __syncwarp();  // lane 0's acquire orders the other lanes' copies
+      const bool go = v >= pre->target;
+      if (go) {
+        constexpr int per_row = NB * (int)sizeof(S) / 16, elems = 16 / (int)sizeof(S);
+        for (int c = lane; c < NB * per_row; c += 32) {
+          const int r = c / per_row, cc = (c % per_row) * elems;
+          cp_async16(pre->dst + r * LDA + cc, pre->src + (size_t)r * pre->ld + cc);
+        }
+      }
+      if (lane == 0) *pre->ready = go ? 1 : 0;
+    }
     if (warp < 2) {
       // the diagonal block, in every lane (upper entries are not used)
       T l[8][8];
@@ -862,10 +896,13 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
   }
   double* Rinv64 = fs64 + 2 * NB * Strip<double>::PB;
   double* XL = fs64;
+  __shared__ int s_in;  // A(k+1, k) staged into Cn during F(k)
   const int nt = a.nt;
   bool pf = false;  // A_kk prefetched into sA
   for (int k = 0; k < nt; ++k) {
     T acc[16];
+    const SolveInput<T> pre{a.upd + (k + 1) * nt + k, k, tile<T>(a, k + 1, k), a.ld, Cn, &s_in};
+    const SolveInput<T>* ppre = k + 1 < nt ? &pre : nullptr;
     // F(k): A_kk after updates 0 .. k-2 (other CTAs), minus L(k,k-1) L(k,k-1)^T
     TRACE(0, a.ntasks + 2 * k);
     TRACE(3, a.ntasks + 2 * k);
@@ -884,7 +921,7 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
     }
     TRACE(1, a.ntasks + 2 * k);
     if constexpr (sizeof(T) == 8) {
-      factor_tile<double, double, false>(a, k, acc, fs64, Lk64, nullptr);
+      factor_tile<double, double, false>(a, k, acc, fs64, Lk64, nullptr, ppre);
     } else {
       double acc64[16];
 #pragma unroll
@@ -892,7 +929,7 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
 #pragma unroll
         for (int cs = 0; cs < 8; ++cs)
           acc64[TileMMA<double>::idx(rs, cs)] = (double)acc[TileMMA<float>::idx(rs, cs)];
-      factor_tile<double, float, false>(a, k, acc64, fs64, Lk64, nullptr);
+      factor_tile<double, float, false>(a, k, acc64, fs64, Lk64, nullptr, ppre);
     }
     publish(a.fin + k * nt + k, 1);
     TRACE(2, a.ntasks + 2 * k);
@@ -906,9 +943,11 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
     // S(k+1, k): A(k+1,k) after updates 0 .. k-1 (other CTAs), times inv(L_kk)^T
     TRACE(0, a.ntasks + 2 * k + 1);
     TRACE(3, a.ntasks + 2 * k + 1);
+    const bool have_in = s_in != 0;
+    if (have_in) cp_async_wait_all();
     if (threadIdx.x == 0) s_pf = ld_acquire(a.upd + (k + 1) * nt + k + 1) >= k;
     leaf_inverses(Lk64, Rinv64, XL);
-    if (k > 0) {
+    if (k > 0 && !have_in) {
       if (!wait_geq(a, a.upd + (k + 1) * nt + k, k, s_ok)) return;
     } else {
       __syncthreads();
@@ -916,9 +955,11 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
     // thread 0's acquire and the barrier order the prefetch after the updates
     pf = s_pf != 0;
     if (pf) stage_async(tile<T>(a, k + 1, k + 1), a.ld, sA, LDA);
-    load_acc(tile<T>(a, k + 1, k), a.ld, acc);
+    if (!have_in) {
+      load_acc(tile<T>(a, k + 1, k), a.ld, acc);
+      acc_to_smem(acc, Cn);
+    }
     TRACE(1, a.ntasks + 2 * k + 1);
-    acc_to_smem(acc, Cn);
     __syncthreads();  // each warp solves rows that other warps stored
     if constexpr (sizeof(T) == 8) trsm_rows<T>(Lk64, XL, Cn, reinterpret_cast<double*>(Cn));
     else trsm_rows<T>(Lk64, XL, Cn, W64);
