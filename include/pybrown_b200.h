@@ -281,6 +281,9 @@ PBG_API int pbg_step_begin(pbg_system *sys, double dt, int build_Dff, int build_
  * the move was accepted (the call synchronises the stream). */
 PBG_API int pbg_step_attempt(pbg_system *sys, const double *xi, int *accepted_host, void *stream);
 PBG_API int pbg_step_end(pbg_system *sys, void *stream);
+/* pbg_step_end, and the wrapped positions (N*3 doubles) copied to host memory
+ * pos_host within the same synchronisation (one wait instead of two). */
+PBG_API int pbg_step_finish(pbg_system *sys, double *pos_host, void *stream);
 
 /* Multi-step run: steps j0 .. j0+n_steps-1 with the build cadence of
  * BD.py:177 (j % diff_freq == 0 ...), each step as Box.propagate does it.

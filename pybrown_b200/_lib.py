@@ -128,6 +128,7 @@ _SIGNATURES = {
     "pbg_step_begin": (_i, [_vp, _d, _i, _i, _i, _vp]),
     "pbg_step_attempt": (_i, [_vp, _vp, _ip, _vp]),
     "pbg_step_end": (_i, [_vp, _vp]),
+    "pbg_step_finish": (_i, [_vp, _vp, _vp]),
     "pbg_run": (_i, [_vp, _ll, _i, _d, _i, _i, _i, _vp, _ll, _vp]),
     "pbg_run_report": (_i, [_vp, ctypes.POINTER(PbgStepReport), _vp]),
     "pbg_batch_create": (_i, [ctypes.POINTER(PbgParams), ctypes.POINTER(_vp)]),

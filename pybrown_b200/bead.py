@@ -10,6 +10,14 @@ import numpy as np
 
 from ._lib import dptr, iptr, lib
 
+_radius_generation = [0]
+
+
+def radius_generation():
+    """Counter bumped whenever any Bead's radius is set (lets a Box skip
+    re-reading every radius before each step)."""
+    return _radius_generation[0]
+
 
 class Bead:
     """Spherical bead (bead.py:30-213): centre `r`, hydrodynamic radius `a`,
@@ -28,6 +36,21 @@ class Bead:
         self.bonded_how = {}
         self.angled_with = []
         self.angled_how = {}
+
+    @property
+    def a(self):
+        return self._a
+
+    @a.setter
+    def a(self, value):
+        self._a = value
+        _radius_generation[0] += 1
+
+    def __setstate__(self, state):
+        # pickles written before `a` became a property hold it as a plain attribute
+        if "a" in state:
+            state["_a"] = state.pop("a")
+        self.__dict__.update(state)
 
     def translate(self, vector):
         """bead.py:92-101."""

@@ -34,8 +34,8 @@ import numpy as np
 from scipy.constants import Boltzmann
 
 from . import _lib
-from .bead import (build_connection_matrix, check_overlaps, compute_pointer_immobile_pbc_matrix,
-                   compute_pointer_pbc_matrix)
+from .bead import (Bead, build_connection_matrix, check_overlaps, compute_pointer_immobile_pbc_matrix,
+                   compute_pointer_pbc_matrix, radius_generation)
 from .interactions import DeviceInteractions, eV_to_joule, kcal_per_mole_to_joule, set_custom_interactions, to_joule
 
 __all__ = ["Box", "eV_to_joule", "kcal_per_mole_to_joule"]
@@ -166,6 +166,10 @@ class Box:
         for i, b in enumerate(mob):
             b.r = self._pos[i]
         self._radii = np.ascontiguousarray([b.a for b in mob], dtype=np.float64)
+        self._pos_synced = self._pos.copy()  # positions the device holds
+        self._radius_gen = radius_generation()
+        self._own_beads = all(type(b) is Bead for b in mob)
+        self._force_key = None
         if N == 0:
             return  # box.py:176: nothing moves
         handle = _lib.ctypes.c_void_p()
@@ -227,8 +231,8 @@ class Box:
             assert count_move_attempts < self.inp["max_move_attempts"], \
                 "maximal number of move attepts exceeded"
         self.last_move_attempts = count_move_attempts
-        _lib.call("pbg_step_end", h, st)
-        _lib.call("pbg_get_positions", h, self._pos.ctypes.data, st)
+        _lib.call("pbg_step_finish", h, self._pos.ctypes.data, st)
+        self._pos_synced[...] = self._pos
         if self.inp["verbose"]:
             print("move attempts: {}".format(count_move_attempts))
 
@@ -239,12 +243,18 @@ class Box:
 
     def _prepare_external_force(self):
         """box.py:452-460."""
-        self.F = np.array(list(self.Fex) * (len(self.mobile_beads)))
+        self.F = np.tile(np.asarray(self.Fex, dtype=float), len(self.mobile_beads))
 
     def _compute_forces(self):
         """box.py:404-428.  The external force and the custom interactions are
         summed here; pbg_step_begin adds the built-in interactions."""
         self.E = 0.0
+        if not self.custom_interactions:
+            # the base force depends on Fex and the unit only: upload it when they change
+            key = (np.asarray(self.Fex, dtype=float).tobytes(), self.inp["energy_unit"])
+            if key == self._force_key:
+                return
+            self._force_key = key
         self._prepare_external_force()
         if self.custom_interactions:
             rij = compute_pointer_pbc_matrix(self.mobile_beads, self.box_length)
@@ -265,13 +275,21 @@ class Box:
         return check_overlaps(self.beads, self.box_length, self.inp["overlap_treshold"], self.connection_matrix)
 
     def _upload_positions(self):
-        radii = [b.a for b in self.mobile_beads]
-        if not np.array_equal(radii, self._radii):
-            self._radii = np.ascontiguousarray(radii, dtype=np.float64)
-            _lib.call("pbg_set_state", self._h, self._pos.ctypes.data, self._radii.ctypes.data,
-                      self._conn.ctypes.data if self._conn is not None else None, self._stream)
-        else:
+        """Sends what the caller changed since the last step: radii (rarely;
+        a Bead bumps a counter when its radius is set) and positions."""
+        gen = radius_generation()
+        if gen != self._radius_gen or not self._own_beads:
+            self._radius_gen = gen
+            radii = [b.a for b in self.mobile_beads]
+            if not np.array_equal(radii, self._radii):
+                self._radii = np.ascontiguousarray(radii, dtype=np.float64)
+                _lib.call("pbg_set_state", self._h, self._pos.ctypes.data, self._radii.ctypes.data,
+                          self._conn.ctypes.data if self._conn is not None else None, self._stream)
+                self._pos_synced[...] = self._pos
+                return
+        if not np.array_equal(self._pos, self._pos_synced):
             _lib.call("pbg_set_positions", self._h, self._pos.ctypes.data, self._stream)
+            self._pos_synced[...] = self._pos
 
     def sync_positions_from_beads(self):
         """Re-link Bead.r to the box after a caller replaced a bead's r array."""
@@ -348,8 +366,8 @@ class Box:
     def __getstate__(self):
         """Restart files (output.py:72-84) carry the device state as host arrays."""
         state = {k: v for k, v in self.__dict__.items()
-                 if k not in ("_h", "_stream", "_pos", "_device_force", "_device_interactions",
-                              "custom_interactions", "interactions")}
+                 if k not in ("_h", "_stream", "_pos", "_pos_synced", "_device_force", "_device_interactions",
+                              "custom_interactions", "interactions", "_force_key")}
         mats = {"D": self.D, "B": self.B}
         if self.hydrodynamics in ("rpy_lub", "rpy_smith_lub"):
             mats.update(Mff=self.Mff, Rff=self.Rff, R=self.R)

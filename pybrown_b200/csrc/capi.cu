@@ -418,6 +418,11 @@ int pbg_step_end(pbg_system* sys, void* stream) {
   return pbg::step_end(sys, (cudaStream_t)stream);
 }
 
+int pbg_step_finish(pbg_system* sys, double* pos_host, void* stream) {
+  if (!sys || !pos_host) return PBG_ERR_ARG;
+  return pbg::step_end(sys, (cudaStream_t)stream, pos_host);
+}
+
 int pbg_run(pbg_system* sys, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
             const double* pool, long long pool_len, void* stream) {
   if (!sys) return PBG_ERR_ARG;

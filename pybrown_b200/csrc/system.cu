@@ -99,6 +99,7 @@ void destroy_system(pbg_system* s) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
+  if (s->hpos) cudaFreeHost(s->hpos);
   delete s;
 }
 
@@ -526,7 +527,7 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
   return PBG_OK;
 }
 
-int step_end(pbg_system* s, cudaStream_t st) {
+int step_end(pbg_system* s, cudaStream_t st, double* pos_out) {
   if (!s->in_step) {
     pbg_set_error_message("pbg_step_end outside a step");
     return PBG_ERR_STATE;
@@ -534,9 +535,18 @@ int step_end(pbg_system* s, cudaStream_t st) {
   s->in_step = false;
   int rc = launch_wrap(s->pos, s->n, s->p.box_length, st);
   if (rc) return rc;
+  const size_t pos_bytes = (size_t)s->N * 3 * sizeof(double);
+  if (pos_out && !s->hpos && cudaMallocHost((void**)&s->hpos, pos_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    s->hpos = nullptr;
+    pbg_set_error_message("cudaMallocHost of the position staging buffer failed");
+    return PBG_ERR_NOMEM;
+  }
+  if (pos_out) PBG_CUDA_TRY(cudaMemcpyAsync(s->hpos, s->pos, pos_bytes, cudaMemcpyDeviceToHost, st));
   // surface factorisation failures of this step
   PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (pos_out) std::memcpy(pos_out, s->hpos, pos_bytes);
   if (s->hflags[1] < 0 || s->hflags[2] < 0 || s->hflags[3] < 0) {
     pbg_set_error_message("a device-wide wait in the factorisation gave up");
     return PBG_ERR_BARRIER;

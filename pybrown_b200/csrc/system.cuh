@@ -37,6 +37,7 @@ struct pbg_system {
   bool divergence = false;     // divergence term of the lubricated D (Ermak scheme)
   double* div = nullptr;       // ld: its value this step
   int* hflags = nullptr;       // pinned mirror
+  double* hpos = nullptr;      // pinned N x 3 staging for pbg_step_finish
 
   // Immobile beads (box.py:649-668): overlap partners and force sources only.
   int M = 0;
@@ -69,7 +70,7 @@ int decompose(pbg_system* s, cudaStream_t st);
 int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st);
 int set_divergence(pbg_system* s, bool on);
 int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st);
-int step_end(pbg_system* s, cudaStream_t st);
+int step_end(pbg_system* s, cudaStream_t st, double* pos_out = nullptr);
 int run(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
         const double* pool, long long pool_len, cudaStream_t st);
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
