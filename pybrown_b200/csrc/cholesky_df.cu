@@ -973,6 +973,24 @@ __device__ void run_chain(const DFArgs& a, unsigned char* smem, int* s_ok) {
   }
 }
 
+// U(i, j, k) with every tile moved by 16-byte copies: the target tile is
+// staged into sC with cp.async together with L_ik, L_jk (instead of per-thread
+// 4-byte loads), updated in registers, and written back through sC with
+// 16-byte stores.  sC: a third [64][LDA] tile.
+template <typename T>
+__device__ __forceinline__ void update_tile(const DFArgs& a, int i, int j, int k, T acc[16], T* sA, T* sB, T* sC) {
+  stage_async(tile<T>(a, i, k), a.ld, sA, LDA);
+  if (i != j) stage_async(tile<T>(a, j, k), a.ld, sB, LDA);
+  stage_async(tile<T>(a, i, j), a.ld, sC, LDA);
+  cp_async_wait_all();
+  __syncthreads();
+  smem_to_acc(sC, acc);
+  TileMMA<T>::sub(sA, i != j ? sB : sA, acc);
+  acc_to_smem(acc, sC);  // each thread rewrites the elements it read
+  __syncthreads();
+  store_tile(sC, LDA, tile<T>(a, i, j), a.ld);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1020,8 +1038,7 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
       const int tg[3] = {1, 1, k};
       if (!wait_all(a, fl, tg, 3, &s_ok)) return;
       TRACE(1, t);
-      load_and_update(a, i, j, k, acc, sA, sB);
-      store_acc(tile<T>(a, i, j), a.ld, acc);
+      update_tile(a, i, j, k, acc, sA, sB, sB + NB * LDA);
       publish(a.upd + i * nt + j, k + 1);
       TRACE(2, t);
     } else {
