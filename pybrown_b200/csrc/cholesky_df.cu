@@ -1120,8 +1120,12 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
       const int* fl[3] = {a.fin + i * nt + k, a.fin + j * nt + k, a.upd + i * nt + j};
       const int tg[3] = {1, 1, k};
       if (!wait_all(a, fl, tg, 3, &s_ok)) return;
-      load_and_update(a, i, j, k, acc, sA, sB);
-      store_acc(tile<T>(a, i, j), a.ld, acc);
+      if constexpr (sizeof(T) == 4) {
+        update_tile(a, i, j, k, acc, sA, sB, sB + NB * LDA);  // three FP32 tiles fit the FP64 layout
+      } else {
+        load_and_update(a, i, j, k, acc, sA, sB);
+        store_acc(tile<T>(a, i, j), a.ld, acc);
+      }
       publish(a.upd + i * nt + j, k + 1);
     } else {
       const int col = j;
