@@ -60,6 +60,28 @@ def bead_config(seed, N, L, a_lo, a_hi, gap=0.0):
     return pos, radii
 
 
+def lub_workload():
+    """Stokesian dynamics with Jeffrey-Onishi lubrication: 512 beads of radius
+    20 A at volume fraction 0.30 (box edge from the volume fraction), minimum
+    gap 0.05 a at placement, lubrication for surface gaps < 1 a
+    (lubrication_cutoff 0.5 in units of a_i + a_j), Cichocki correction,
+    midpoint scheme (m = 100), dt = 0.1 ps, seed 0."""
+    N, a, phi = 512, 20.0, 0.30
+    L = (N * 4.0 * math.pi * a ** 3 / 3.0 / phi) ** (1.0 / 3.0)
+    return {"workload": "SD N=512 a=20 phi=0.30 rpy_smith_lub JO cutoff 0.5 Cichocki midpoint m=100 dt=0.1",
+            "n_beads": N, "radius": a, "volume_fraction": phi, "box_length": L, "min_gap": 0.05 * a,
+            "lubrication_cutoff": 0.5, "m_midpoint": 100.0, "dt": 0.1, "seed": 0}
+
+
+def lub_input(precision):
+    w = lub_workload()
+    inp = box_input(precision)
+    inp.update({"box_length": w["box_length"], "hydrodynamics": "rpy_smith_lub",
+                "lubrication_cutoff": w["lubrication_cutoff"], "cichocki_correction": True,
+                "propagation_scheme": "midpoint", "m_midpoint": w["m_midpoint"]})
+    return inp
+
+
 def box_input(precision):
     return {"box_length": WORKLOAD["box_length"], "T": 293.15, "viscosity": 0.01005, "seed": 0,
             "hydrodynamics": "rpy_smith", "ewald_alpha": math.sqrt(math.pi),
@@ -136,12 +158,12 @@ class DeviceRun:
     """Device-resident stepping through the C ABI: state, D, B and the noise
     pool live in HBM; one pbg_step_begin / attempt / end per step."""
 
-    def __init__(self, pos, radii, precision, n_noise_steps, seed, torch):
+    def __init__(self, pos, radii, precision, n_noise_steps, seed, torch, inp=None):
         from pybrown_b200 import _lib
         from pybrown_b200.bead import Bead
         from pybrown_b200.box import Box
         self._lib, self.torch = _lib, torch
-        self.box = Box([Bead(p, a) for p, a in zip(pos, radii)], box_input(precision))
+        self.box = Box([Bead(p, a) for p, a in zip(pos, radii)], inp or box_input(precision))
         self.n = 3 * len(radii)
         rs = np.random.RandomState(seed)
         self.pool = torch.tensor(rs.normal(0.0, 1.0, size=(n_noise_steps + 64) * self.n), dtype=torch.float64,
@@ -360,11 +382,39 @@ def run_ours(args, torch, dist, rank, world):
         "cpu_baseline": cpu,
         "clocks": results["mixed"]["clocks"],
     }
+    if world == 1 and not args.no_lub:
+        line["lubrication"] = run_lub_section(args, torch)
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch_section(args, torch)
     if world == 1 and not args.no_serve:
         line["serve"] = run_serve_section(args, torch)
     return line
+
+
+def run_lub_section(args, torch, precisions=("fp64", "mixed")):
+    """The lubricated workload (lub_workload) stepped on the device: per-step
+    CUDA events with an L2 flush between steps, like the main workload."""
+    w = lub_workload()
+    pos, radii = bead_config(w["seed"], w["n_beads"], w["box_length"], w["radius"], w["radius"], gap=w["min_gap"])
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {"workload": w["workload"], "box_length": w["box_length"], "steps": args.steps}
+    runs = {}
+    for prec in precisions:
+        run = DeviceRun(pos, radii, prec, 4 * (args.warmup + args.steps) + 64, w["seed"], torch, inp=lub_input(prec))
+        for _ in range(args.warmup):
+            run.step(w["dt"])
+        torch.cuda.synchronize()
+        ms = timed_steps(torch, lambda: run.step(w["dt"]), args.steps, flush)
+        runs[prec] = run
+        out[prec] = {"ms_per_step": ms / args.steps, "steps_per_s": args.steps / (ms * 1e-3),
+                     "move_attempts": run.cursor}
+    if "fp64" in runs and "mixed" in runs:
+        d_ref = runs["fp64"].positions() - pos
+        d_mix = runs["mixed"].positions() - pos
+        d_mix -= w["box_length"] * np.round((d_mix - d_ref) / w["box_length"])
+        out["mixed_vs_fp64_displacement_rel_err"] = float(np.max(np.abs(d_mix - d_ref)) / np.max(np.abs(d_ref)))
+        out["mixed_over_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    return out
 
 
 def run_batch_section(args, torch):
@@ -383,6 +433,7 @@ def run_batch_section(args, torch):
         batch.add(place_beads(rng, radii, L), radii, L, seed=k, noise="device")
     for _ in range(args.warmup):
         batch.propagate(0.5)
+    tune = batch.autotune(reps=2)  # schedule of the batched factorisation (results unchanged)
     torch.cuda.synchronize()
     launches0 = _lib.lib.pbg_launch_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -399,7 +450,9 @@ def run_batch_section(args, torch):
                         "mixed, dt=0.5, device Philox noise", "replicas": 256, "beads": beads,
             "steps": args.steps, "ms_per_step": ms / args.steps,
             "bead_steps_per_s": beads * args.steps / (ms * 1e-3),
-            "replica_steps_per_s": 256 * args.steps / (ms * 1e-3), "gpu_launches_per_step": launches}
+            "replica_steps_per_s": 256 * args.steps / (ms * 1e-3), "gpu_launches_per_step": launches,
+            "schedule": {"merge_order": tune["merge_order"], "ctas_per_sm": tune["ctas_per_sm"],
+                         "factorisation_ms": {f"{o}/{c}": round(v, 4) for (o, c), v in tune["ms"].items()}}}
 
 
 def run_serve_section(args, torch):
@@ -446,6 +499,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-lub", action="store_true", help="skip the lubricated (Stokesian dynamics) section")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving stream")

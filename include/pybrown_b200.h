@@ -341,6 +341,20 @@ PBG_API int pbg_batch_step_end(pbg_batch *b, int *status, void *stream);
 /* D or B (PBG_MAT_D / PBG_MAT_B) of one replica, 3N x 3N FP64 row-major host array. */
 PBG_API int pbg_batch_get_matrix(pbg_batch *b, int slot, int which, double *out);
 
+/* Schedule of the batched factorisation (no counterpart in the reference).
+ * merge_order: how the replicas' task segments are interleaved in the one
+ * task list; ctas_per_sm: resident CTAs per SM of the persistent kernel
+ * (0 = as many as fit).  No choice changes any result bit. */
+enum { PBG_MERGE_LARGER_FIRST = 0, PBG_MERGE_ADDED = 1, PBG_MERGE_SMALLER_FIRST = 2, PBG_MERGE_REPLICA_MAJOR = 3 };
+PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_sm);
+/* Autotuner: after a step has built D (not inside a step), times `reps`
+ * factorisations of the current matrices under every schedule (the four
+ * merge orders x 1 or 2 CTAs per SM in FP32, 1 in FP64), keeps the fastest
+ * and leaves B as the factor of the current D (the value a step would give).
+ * best[2] = {merge_order, ctas_per_sm}; ms (may be NULL) receives the mean
+ * time of each candidate, merge order major (8 entries). */
+PBG_API int pbg_batch_autotune(pbg_batch *b, int reps, int *best, float *ms, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

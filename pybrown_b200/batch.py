@@ -127,6 +127,25 @@ class ReplicaBatch:
     def last_move_attempts(self, slot):
         return self._rep[slot]["last_move_attempts"]
 
+    # ---------------------------------------------------------------- schedule
+    MERGE_ORDERS = ("larger_first", "added", "smaller_first", "replica_major")
+
+    def set_schedule(self, merge_order="larger_first", ctas_per_sm=0):
+        """Schedule of the batched factorisation: the interleaving of the
+        replicas' task segments and the resident CTAs per SM (0 = as many as
+        fit).  No choice changes a result."""
+        _lib.call("pbg_batch_set_schedule", self._h, self.MERGE_ORDERS.index(merge_order), int(ctas_per_sm))
+
+    def autotune(self, reps=3):
+        """Times the factorisation of the current matrices under every
+        schedule (after a step, between steps), keeps the fastest and returns
+        {"merge_order", "ctas_per_sm", "ms": {(merge_order, ctas): mean ms}}."""
+        best = (ctypes.c_int * 2)()
+        ms = (ctypes.c_float * 8)()
+        _lib.call("pbg_batch_autotune", self._h, int(reps), best, ms, self._stream)
+        table = {(self.MERGE_ORDERS[k // 2], k % 2 + 1): float(ms[k]) for k in range(8) if ms[k] >= 0}
+        return {"merge_order": self.MERGE_ORDERS[best[0]], "ctas_per_sm": int(best[1]), "ms": table}
+
     # ---------------------------------------------------------------- step
     def propagate(self, dt, build_D=True, cholesky=True):
         """One step of every replica (box.py:150-250, Ermak scheme)."""

@@ -121,6 +121,12 @@ struct pbg_batch {
   std::vector<unsigned char> mask;  // of the last upload, active order
   size_t cap = 0;  // capacity of the per-replica device/pinned arrays
   int max_n = 0;
+  // Schedule of the batched factorisation (pbg_batch_autotune): the order in
+  // which the replicas' task segments are merged, and the resident CTAs per
+  // SM (0 = as many as fit).  Neither changes any result.
+  int merge_order = PBG_MERGE_LARGER_FIRST;
+  int ctas_per_sm = 0;
+  bool have_D = false;  // a step has built D (the autotuner factors it)
 };
 
 namespace pbg {
@@ -432,23 +438,38 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
     c.nt = r->nt;
     c.pad = 0;
   }
-  // merge order: segment number, then larger matrices first (see cholesky_df.cu)
+  // Merge order of the replicas' task segments (see cholesky_df.cu): by
+  // segment number with larger matrices first (default), in the order the
+  // replicas were added, smaller first, or replica after replica (all of
+  // one replica's segments, larger replicas first).  Each replica's own
+  // segments keep their order in every policy, so every task still depends
+  // only on earlier tasks.
   std::vector<int> order(R);
   for (int q = 0; q < R; ++q) order[q] = q;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return b->slots[b->active[x]]->nt > b->slots[b->active[y]]->nt;
-  });
+  if (b->merge_order != PBG_MERGE_ADDED) {
+    const bool larger = b->merge_order != PBG_MERGE_SMALLER_FIRST;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+      const int nx = b->slots[b->active[x]]->nt, ny = b->slots[b->active[y]]->nt;
+      return larger ? nx > ny : nx < ny;
+    });
+  }
   std::vector<GatherSeg> segs;
   long long dst = 0;
-  for (int sg = 0; sg < max_seg; ++sg)
-    for (int q : order) {
-      const BatchReplica* r = b->slots[b->active[q]];
-      if (sg + 1 >= (int)r->seg_start.size()) continue;
-      const int count = r->seg_start[sg + 1] - r->seg_start[sg];
-      if (count <= 0) continue;
-      segs.push_back(GatherSeg{r->tasks + r->seg_start[sg], dst, count, q});
-      dst += count;
-    }
+  auto push_seg = [&](int q, int sg) {
+    const BatchReplica* r = b->slots[b->active[q]];
+    if (sg + 1 >= (int)r->seg_start.size()) return;
+    const int count = r->seg_start[sg + 1] - r->seg_start[sg];
+    if (count <= 0) return;
+    segs.push_back(GatherSeg{r->tasks + r->seg_start[sg], dst, count, q});
+    dst += count;
+  };
+  if (b->merge_order == PBG_MERGE_REPLICA_MAJOR) {
+    for (int q : order)
+      for (int sg = 0; sg < max_seg; ++sg) push_seg(q, sg);
+  } else {
+    for (int sg = 0; sg < max_seg; ++sg)
+      for (int q : order) push_seg(q, sg);
+  }
   if ((rc = ensure(b->d_reps, b->cap_reps, R * sizeof(BatchDev))) ||
       (rc = ensure(b->d_rpy, b->cap_rpy, rpy.size())) ||
       (rc = ensure(b->d_ework, b->cap_ework, n_ework * sizeof(int4))) ||
@@ -747,8 +768,10 @@ PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int chole
     else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
     PBG_CHECK_LAUNCH();
     PBG_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st));
-    if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, st))) return rc;
+    if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, b->ctas_per_sm, st)))
+      return rc;
   }
+  if (build_D) b->have_D = true;
   bool any_force = false;
   for (int s : b->active) any_force = any_force || b->slots[s]->has_force;
   if (any_force) {
@@ -834,6 +857,91 @@ PBG_API int pbg_batch_step_end(pbg_batch* b, int* status, void* stream) {
 
 // D or B (which = PBG_MAT_D / PBG_MAT_B) of one replica as a 3N x 3N FP64
 // row-major host array.
+PBG_API int pbg_batch_set_schedule(pbg_batch* b, int merge_order, int ctas_per_sm) {
+  if (!b || merge_order < PBG_MERGE_LARGER_FIRST || merge_order > PBG_MERGE_REPLICA_MAJOR || ctas_per_sm < 0)
+    return PBG_ERR_ARG;
+  if (b->in_step) {
+    pbg_set_error_message("pbg_batch_set_schedule inside a step");
+    return PBG_ERR_STATE;
+  }
+  if (merge_order != b->merge_order) b->dirty = true;
+  b->merge_order = merge_order;
+  b->ctas_per_sm = ctas_per_sm;
+  return PBG_OK;
+}
+
+// Times the copy of D into B and the batched factorisation under each
+// schedule.  Refactoring the current D reproduces the current B bit for bit
+// (every tile's arithmetic is fixed by the task order of its replica).
+PBG_API int pbg_batch_autotune(pbg_batch* b, int reps, int* best, float* ms, void* stream) {
+  if (!b || reps < 1 || !best) return PBG_ERR_ARG;
+  if (b->in_step || !b->have_D) {
+    pbg_set_error_message("pbg_batch_autotune needs a completed step and must be called between steps");
+    return PBG_ERR_STATE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int R = (int)b->active.size();
+  const bool f64 = b->precision == PBG_PREC_FP64;
+  const int max_ctas = f64 ? 1 : 2;
+  if (ms)
+    for (int c = 0; c < 8; ++c) ms[c] = -1.0f;
+  const int old_order = b->merge_order, old_ctas = b->ctas_per_sm;
+  float best_ms = -1.0f;
+  best[0] = old_order;
+  best[1] = old_ctas;
+  cudaEvent_t e0, e1;
+  PBG_CUDA_TRY(cudaEventCreate(&e0));
+  PBG_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = PBG_OK;
+  for (int order = PBG_MERGE_LARGER_FIRST; order <= PBG_MERGE_REPLICA_MAJOR && rc == PBG_OK && R; ++order) {
+    for (int ctas = 1; ctas <= max_ctas && rc == PBG_OK; ++ctas) {
+      b->merge_order = order;
+      b->ctas_per_sm = ctas;
+      b->dirty = true;
+      if ((rc = rebuild(b, st))) break;
+      float total = 0.0f;
+      for (int r = 0; r <= reps && rc == PBG_OK; ++r) {  // the first run is a warm-up
+        if (cudaEventRecord(e0, st) != cudaSuccess) { rc = PBG_ERR_CUDA; break; }
+        const dim3 g(64, R);
+        if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
+        else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+        if (cudaGetLastError() != cudaSuccess) { rc = PBG_ERR_CUDA; break; }
+        pbg_count_launch();
+        if (cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st) != cudaSuccess) { rc = PBG_ERR_CUDA; break; }
+        if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, ctas, st))) break;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) { rc = PBG_ERR_CUDA; break; }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (r) total += t;
+      }
+      if (rc != PBG_OK) break;
+      const float mean = total / reps;
+      if (ms) ms[order * 2 + ctas - 1] = mean;
+      if (best_ms < 0.0f || mean < best_ms) {
+        best_ms = mean;
+        best[0] = order;
+        best[1] = ctas;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->merge_order = rc == PBG_OK ? best[0] : old_order;
+  b->ctas_per_sm = rc == PBG_OK ? best[1] : old_ctas;
+  b->dirty = true;
+  if (rc == PBG_OK) {
+    // surface a failed factorisation like a step would
+    PBG_CUDA_TRY(cudaMemcpyAsync(b->h_info, b->d_info, R * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int q = 0; q < R; ++q)
+      if (b->h_info[q] != 0) {
+        pbg_set_error_message("factorisation failed during autotuning (replica %d, info %d)", q, b->h_info[q]);
+        return b->h_info[q] < 0 ? PBG_ERR_BARRIER : PBG_ERR_NOT_SPD;
+      }
+  }
+  return rc;
+}
+
 PBG_API int pbg_batch_get_matrix(pbg_batch* b, int slot, int which, double* out) {
   BatchReplica* r = slot_of(b, slot);
   if (!r || !out || (which != PBG_MAT_D && which != PBG_MAT_B)) return PBG_ERR_ARG;

@@ -1407,7 +1407,7 @@ void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& 
 }
 
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
-                          cudaStream_t st) {
+                          int ctas_per_sm, cudaStream_t st) {
   if (ntasks <= 0) return PBG_OK;
   const bool f64 = precision == PBG_PREC_FP64;
   const size_t smem = f64 ? batch_smem_bytes<double>() : batch_smem_bytes<float>();
@@ -1431,7 +1431,7 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
       return PBG_ERR_CUDA;
     }
   }
-  int grid = num_sms * bps;
+  int grid = num_sms * (ctas_per_sm > 0 ? std::min(ctas_per_sm, bps) : bps);
   if (grid > ntasks) grid = ntasks;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
@@ -1445,6 +1445,251 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
   cfg.numAttrs = 1;
   if (f64) PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<double>, reps, tasks, ntasks, ctl));
   else PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<float>, reps, tasks, ntasks, ctl));
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+
+// ---------------------------------------------------------------- SPD inverse on the tensor cores
+// inv(A) = X^T X with A = L L^T (the data-flow factorisation above) and
+// X = inv(L): X by a right-looking blocked solve of L X = I, one launch per
+// block row k (X_i. -= L_ik X_k. for every i > k, row k+1 finished with
+// inv(L_{k+1,k+1}) in the same launch) -- and X^T X with one CTA per lower
+// tile.  Every tile product is
+// TileMMA: FP64 DMMA for FP64 matrices, 3xTF32 split products with FP32
+// accumulation for FP32 ones.  Used by the SPD inverse of the FP64
+// lubrication path (cholesky.cu) and by the mixed lubricated path, which also
+// reads the factor of kBT inv(R) off X (tc_reversed_factor).
+//
+// Mixed workspace (tc_inverse_work_bytes): [inv(L_kk) tiles][data-flow
+// scratch][X: ld x ld][F: ld x ld], F the matrix to factor (in place).
+
+namespace {
+
+template <typename T>
+constexpr size_t tc_smem_bytes() {
+  return 2 * NB * LDA * sizeof(T);
+}
+
+// s[c][r] = g[r][c] for a 64 x 64 tile (rows of LDA in smem).
+template <typename T>
+__device__ __forceinline__ void stage_transposed(const T* __restrict__ g, int ld, T* s) {
+  for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
+    const int r = e >> 6, c = e & 63;
+    s[c * LDA + r] = g[(size_t)r * ld + c];
+  }
+}
+
+// inv(L_kk) with its upper triangle zeroed, into smem rows of LDA.
+template <typename T>
+__device__ __forceinline__ void stage_invdiag(const T* __restrict__ invdiag, int k, T* s) {
+  const T* inv = invdiag + (size_t)k * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
+    const int r = e >> 6, c = e & 63;
+    s[r * LDA + c] = c <= r ? inv[e] : T(0);
+  }
+}
+
+// Step k of the blocked solve L X = I (launched for k = -1 .. nt-2), with
+// block row k of X final on entry: CTA (i, c), i = k+1 .. nt-1, c = 0 .. k,
+// applies X_ic -= L_ik X_kc; the CTAs of row k+1 then finish that row,
+// X_{k+1,c} = inv(L_{k+1,k+1}) X_{k+1,c}, and the last CTA writes the
+// diagonal tile X_{k+1,k+1} = inv(L_{k+1,k+1}).  Rows > k+1 read only row k,
+// which nobody writes in this launch.
+template <typename T>
+__global__ void __launch_bounds__(THREADS) trsm_step_kernel(const T* __restrict__ L, const T* __restrict__ invdiag,
+                                                            int k, T* X, int ld, int nt) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* sA = reinterpret_cast<T*>(smem);
+  T* sB = sA + NB * LDA;
+  const int nupd = (nt - k - 1) * (k + 1);
+  if ((int)blockIdx.x == nupd) {
+    T* g = X + (size_t)(k + 1) * NB * ld + (size_t)(k + 1) * NB;
+    const T* inv = invdiag + (size_t)(k + 1) * NB * NB;
+    for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
+      const int r = e >> 6, c = e & 63;
+      g[(size_t)r * ld + c] = c <= r ? inv[e] : T(0);
+    }
+    return;
+  }
+  const int i = k + 1 + blockIdx.x / (k + 1), c = blockIdx.x % (k + 1);
+  stage_async(L + (size_t)i * NB * ld + (size_t)k * NB, ld, sA, LDA);
+  stage_transposed(X + (size_t)k * NB * ld + (size_t)c * NB, ld, sB);
+  T* Xic = X + (size_t)i * NB * ld + (size_t)c * NB;
+  T acc[16];
+  load_acc(Xic, ld, acc);
+  cp_async_wait_all();
+  __syncthreads();
+  TileMMA<T>::sub(sA, sB, acc);
+  if (i == k + 1) {
+    __syncthreads();  // sA, sB free
+#pragma unroll
+    for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+      for (int cs = 0; cs < 8; ++cs) sB[acc_col(cs) * LDA + acc_row(rs)] = acc[TileMMA<T>::idx(rs, cs)];
+    stage_invdiag(invdiag, k + 1, sA);
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = T(0);
+    TileMMA<T>::sub(sA, sB, acc);  // acc = -inv(L_{k+1,k+1}) X_{k+1,c}
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
+  }
+  store_acc(Xic, ld, acc);
+}
+
+// out_IJ = scale (X^T X)_IJ = scale sum_{k >= I} X_kI^T X_kJ for the lower
+// tile (I, J), written to (I, J) and (J, I); with `reversed` every element
+// (r, c) goes to (ld-1-r, ld-1-c) instead.
+template <typename T>
+__global__ void __launch_bounds__(THREADS) lauum_tc_kernel(const T* __restrict__ X, int ld, int nt, T scale,
+                                                           int reversed, T* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* sA = reinterpret_cast<T*>(smem);
+  T* sB = sA + NB * LDA;
+  const int b = blockIdx.x;
+  int I = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+  while ((I + 1) * (I + 2) / 2 <= b) ++I;
+  while (I * (I + 1) / 2 > b) --I;
+  const int J = b - I * (I + 1) / 2;
+  T acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  for (int k = I; k < nt; ++k) {
+    stage_transposed(X + (size_t)k * NB * ld + (size_t)I * NB, ld, sA);
+    stage_transposed(X + (size_t)k * NB * ld + (size_t)J * NB, ld, sB);
+    __syncthreads();
+    TileMMA<T>::sub(sA, sB, acc);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) {
+      const T v = -acc[TileMMA<T>::idx(rs, cs)] * scale;
+      int r = I * NB + acc_row(rs), c = J * NB + acc_col(cs);
+      if (reversed) {
+        r = ld - 1 - r;
+        c = ld - 1 - c;
+      }
+      out[(size_t)r * ld + c] = v;
+      if (I != J) out[(size_t)c * ld + r] = v;  // a diagonal tile writes each element once
+    }
+}
+
+// B[i][j] = scale X[ld-1-j][ld-1-i] for the lower triangle of B (32 x 32
+// tiles through smem; tiles above the diagonal are not written).
+template <typename T>
+__global__ void reversed_transpose_kernel(const T* __restrict__ X, int ld, T scale, T* __restrict__ B) {
+  __shared__ T t[32][33];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bj > bi) return;
+  const int x0r = ld - 32 * (bj + 1), x0c = ld - 32 * (bi + 1);
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) t[r][threadIdx.x] = X[(size_t)(x0r + r) * ld + x0c + threadIdx.x];
+  __syncthreads();
+  for (int rr = threadIdx.y; rr < 32; rr += blockDim.y)
+    B[(size_t)(bi * 32 + rr) * ld + bj * 32 + threadIdx.x] = scale * t[31 - threadIdx.x][31 - rr];
+}
+
+// inv(B_II) for B = s J G^{-T} J (G lower, order ld, J the reversal of all ld
+// indices): (1/s) J G_I'I'^T J with I' = nt-1-I, from the lower triangle of
+// G's diagonal tile.
+template <typename T>
+__global__ void b_invdiag_kernel(const T* __restrict__ G, int ld, int nt, T inv_scale, T* __restrict__ invdiag) {
+  const int I = blockIdx.x, Ip = nt - 1 - I;
+  const T* g = G + (size_t)Ip * NB * ld + (size_t)Ip * NB;
+  T* o = invdiag + (size_t)I * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    o[e] = r >= c ? inv_scale * g[(size_t)(NB - 1 - c) * ld + (NB - 1 - r)] : T(0);
+  }
+}
+
+// Dynamic shared memory above the 48 KB default (the FP64 tiles), set on the
+// current device before each use.
+template <typename T>
+int set_tc_smem() {
+  constexpr int smem = (int)tc_smem_bytes<T>();
+  PBG_CUDA_TRY(cudaFuncSetAttribute(trsm_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  PBG_CUDA_TRY(cudaFuncSetAttribute(lauum_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  return PBG_OK;
+}
+
+template <typename T>
+int trtri_tc(const T* L, const T* invdiag, T* X, int ld, cudaStream_t st) {
+  const int nt = ld / NB;
+  constexpr size_t smem = tc_smem_bytes<T>();
+  if (int rc = set_tc_smem<T>()) return rc;
+  PBG_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ld * ld * sizeof(T), st));
+  for (int k = -1; k + 1 < nt; ++k) {
+    trsm_step_kernel<T><<<(nt - k - 1) * (k + 1) + 1, THREADS, smem, st>>>(L, invdiag, k, X, ld, nt);
+    PBG_CHECK_LAUNCH();
+  }
+  return PBG_OK;
+}
+
+template <typename T>
+int lauum_tc(const T* X, int ld, T scale, bool reversed, T* out, cudaStream_t st) {
+  const int nt = ld / NB;
+  if (int rc = set_tc_smem<T>()) return rc;
+  lauum_tc_kernel<T><<<nt * (nt + 1) / 2, THREADS, tc_smem_bytes<T>(), st>>>(X, ld, nt, scale, reversed ? 1 : 0,
+                                                                             out);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+}  // namespace
+
+int launch_trtri_tc(const void* L, const void* invdiag, void* X, int ld, int precision, cudaStream_t st) {
+  if (ld % NB != 0 || ld <= 0) return PBG_ERR_ARG;
+  if (precision == PBG_PREC_FP64) return trtri_tc<double>((const double*)L, (const double*)invdiag, (double*)X, ld, st);
+  return trtri_tc<float>((const float*)L, (const float*)invdiag, (float*)X, ld, st);
+}
+
+int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* out, int precision, cudaStream_t st) {
+  if (ld % NB != 0 || ld <= 0) return PBG_ERR_ARG;
+  if (precision == PBG_PREC_FP64) return lauum_tc<double>((const double*)X, ld, scale, reversed, (double*)out, st);
+  return lauum_tc<float>((const float*)X, ld, (float)scale, reversed, (float*)out, st);
+}
+
+size_t tc_inverse_work_bytes(int ld) {
+  const size_t nt = ld / NB;
+  return nt * NB * NB * sizeof(float) + df_work_bytes(ld) + 2 * (size_t)ld * ld * sizeof(float);
+}
+
+TcInverseWork tc_inverse_work(void* work, int ld) {
+  const size_t nt = ld / NB;
+  unsigned char* p = static_cast<unsigned char*>(work);
+  TcInverseWork w;
+  w.invdiag = reinterpret_cast<float*>(p);
+  w.scratch = p + nt * NB * NB * sizeof(float);
+  w.X = reinterpret_cast<float*>(static_cast<unsigned char*>(w.scratch) + df_work_bytes(ld));
+  w.F = w.X + (size_t)ld * ld;
+  return w;
+}
+
+int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st) {
+  if (ld % NB != 0 || ld <= 0) return PBG_ERR_ARG;
+  const TcInverseWork w = tc_inverse_work(work, ld);
+  if (reinterpret_cast<uintptr_t>(w.X) % 16 != 0) {
+    pbg_set_error_message("tensor-core inverse: misaligned workspace");
+    return PBG_ERR_ARG;
+  }
+  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED, info, w.invdiag, w.scratch, st);
+  if (rc != PBG_OK) return rc;
+  return trtri_tc<float>(w.F, w.invdiag, w.X, ld, st);
+}
+
+int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, cudaStream_t st) {
+  return lauum_tc<float>(X, ld, scale, reversed, out, st);
+}
+
+int tc_reversed_factor(const float* X, const float* G, int ld, double s, float* B, float* invdiag,
+                       cudaStream_t st) {
+  const int nt = ld / NB;
+  reversed_transpose_kernel<float><<<dim3(ld / 32, ld / 32), dim3(32, 8), 0, st>>>(X, ld, (float)s, B);
+  PBG_CHECK_LAUNCH();
+  b_invdiag_kernel<float><<<nt, THREADS, 0, st>>>(G, ld, nt, (float)(1.0 / s), invdiag);
   PBG_CHECK_LAUNCH();
   return PBG_OK;
 }

@@ -120,6 +120,29 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
 size_t spd_inverse_work_bytes(int ld);
 int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st);
 
+// X = inv(L) (L lower with its inverted diagonal tiles in invdiag) and
+// out = scale X^T X (optionally with every index i -> ld-1-i), on the tensor
+// cores, FP64 or FP32 (cholesky_df.cu).
+int launch_trtri_tc(const void* L, const void* invdiag, void* X, int ld, int precision, cudaStream_t st);
+int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* out, int precision, cudaStream_t st);
+// SPD inverse of the mixed lubricated path (FP32).  The caller puts the
+// matrix (order ld, padded) in F; tc_factor_invert factors it in place
+// (F = G, lower) and forms X = inv(G); tc_lauum writes scale X^T X;
+// tc_reversed_factor writes B = s J X^T J (lower; J reverses all ld indices)
+// and the inverted diagonal tiles of that B, for launch_trsv_upper.
+struct TcInverseWork {
+  float* invdiag;  // nt x 64 x 64
+  void* scratch;   // data-flow scratch
+  float* X;        // ld x ld
+  float* F;        // ld x ld
+};
+size_t tc_inverse_work_bytes(int ld);
+TcInverseWork tc_inverse_work(void* work, int ld);
+int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st);
+int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, cudaStream_t st);
+int tc_reversed_factor(const float* X, const float* G, int ld, double s, float* B, float* invdiag,
+                       cudaStream_t st);
+
 // Batched factorisation of many independent matrices (one per replica).
 struct CholRep {
   void* A;        // ld x ld, padded with the identity beyond n
@@ -134,8 +157,9 @@ struct CholRep {
 // task.x = type | replica << 2 in the merged list.
 void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start);
 // ctl: 4 ints (next task, abort, spin failures, error bits), zero before the launch.
+// ctas_per_sm: resident CTAs per SM (0 = as many as fit).
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
-                          cudaStream_t st);
+                          int ctas_per_sm, cudaStream_t st);
 
 // Batched RPY / Smith-Ewald tensor build: one argument block per replica and
 // a work list of bead tiles (x = replica, y = I, z = J with I >= J).

@@ -63,6 +63,52 @@ __global__ void export_matrix_kernel(const T* __restrict__ src, int n, int ld, i
 
 inline int grid_for(long long total) { return (int)std::min<long long>((total + 255) / 256, 148LL * 16); }
 
+// ---- mixed lubricated path -------------------------------------------------
+// R = Rff (FP32 -> FP64), every element of the padded matrix.
+__global__ void widen_matrix_kernel(const float* __restrict__ src, double* __restrict__ dst, long long total) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    dst[t] = (double)src[t];
+}
+
+// F = J R J rounded to FP32, J the reversal of all ld indices (the identity
+// padding moves to the leading rows and columns).
+__global__ void reverse_narrow_kernel(const double* __restrict__ R, int ld, float* __restrict__ F) {
+  const long long total = (long long)ld * ld;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    F[t] = (float)R[total - 1 - t];
+}
+
+// res = b - R x in FP64 (one warp per row, fixed shuffle tree).
+__global__ void residual_kernel(const double* __restrict__ R, int ld, int n, const double* __restrict__ b,
+                                const double* __restrict__ x, double* __restrict__ res) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const double* r = R + (size_t)row * ld;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += r[j] * x[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) res[row] = b[row] - s;
+}
+
+// x += y ; out = c (a - b)
+__global__ void add_vec_kernel(double* __restrict__ x, const double* __restrict__ y, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += y[i];
+}
+// out[i] = c in[ld-1-i] (J, the reversal of all ld indices, times c)
+__global__ void reverse_scale_kernel(const double* __restrict__ in, int ld, double c, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ld) out[i] = c * in[ld - 1 - i];
+}
+__global__ void diff_scaled_kernel(const double* __restrict__ a, const double* __restrict__ b, double c, int n,
+                                   double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = c * (a[i] - b[i]);
+}
+
 }  // namespace
 
 template <typename F>
@@ -95,7 +141,8 @@ void destroy_system(pbg_system* s) {
   void* ptrs[] = {s->pos,  s->pos_snap, s->radii, s->conn,  s->force, s->D,     s->B,    s->D0,
                   s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
                   s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
-                  s->chol_work, s->inv_work, s->dflags, s->div};
+                  s->chol_work, s->inv_work, s->dflags, s->div, s->sol, s->sol0, s->res, s->corr,
+                  s->G,    s->Ginv};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
@@ -120,10 +167,13 @@ int create_system(const pbg_params* prm, pbg_system** out) {
   s->ld = pbg_round_up(s->n, PBG_TILE);
   s->lub = p.hydrodynamics == PBG_HI_RPY_LUB || p.hydrodynamics == PBG_HI_RPY_SMITH_LUB;
   s->smith = p.hydrodynamics == PBG_HI_RPY_SMITH || p.hydrodynamics == PBG_HI_RPY_SMITH_LUB;
-  // The lubricated resistance path runs in FP64 (the mixed path covers D and B
-  // of the far-field modes).
-  s->prec = s->lub ? PBG_PREC_FP64 : p.precision;
+  // Lubrication modes with precision "mixed": FP32 far-field mobility and its
+  // tensor-core inverse, FP64 resistance matrix R, FP32 D and B from the
+  // tensor-core inverse of J R J, FP64-refined solves with R.
+  s->mlub = s->lub && p.precision == PBG_PREC_MIXED;
+  s->prec = p.precision;
   s->es = s->prec == PBG_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t ff_es = s->mlub ? sizeof(float) : sizeof(double);
   const size_t N = s->N, ld = s->ld;
   const size_t mat = ld * ld;
   if (s->smith) {
@@ -141,17 +191,22 @@ int create_system(const pbg_params* prm, pbg_system** out) {
   SYS_ALLOC(s->B, mat * s->es);
   if (p.propagation_scheme == PBG_SCHEME_MIDPOINT) SYS_ALLOC(s->D0, mat * s->es);
   if (s->lub) {
-    SYS_ALLOC(s->Mff, mat * sizeof(double));
-    SYS_ALLOC(s->Rff, mat * sizeof(double));
+    SYS_ALLOC(s->Mff, mat * ff_es);
+    SYS_ALLOC(s->Rff, mat * ff_es);
     SYS_ALLOC(s->R, mat * sizeof(double));
     if (p.propagation_scheme == PBG_SCHEME_MIDPOINT) {
-      SYS_ALLOC(s->Mff0, mat * sizeof(double));
-      SYS_ALLOC(s->Rff0, mat * sizeof(double));
+      SYS_ALLOC(s->Mff0, mat * ff_es);
+      SYS_ALLOC(s->Rff0, mat * ff_es);
       SYS_ALLOC(s->R0, mat * sizeof(double));
     }
-    SYS_ALLOC(s->inv_work, spd_inverse_work_bytes(s->ld));
+    SYS_ALLOC(s->inv_work, s->mlub ? tc_inverse_work_bytes(s->ld) : spd_inverse_work_bytes(s->ld));
+    if (s->mlub) {
+      SYS_ALLOC(s->G, mat * sizeof(float));
+      SYS_ALLOC(s->Ginv, (size_t)PBG_TILE * ld * sizeof(float));
+    }
   }
-  double** vecs[] = {&s->FX, &s->U, &s->BX, &s->ddet, &s->y, &s->rwork, &s->Dy, &s->drift, &s->xi};
+  double** vecs[] = {&s->FX, &s->U,  &s->BX,   &s->ddet, &s->y,   &s->rwork, &s->Dy,
+                     &s->drift, &s->xi, &s->sol, &s->sol0, &s->res, &s->corr};
   for (double** v : vecs) SYS_ALLOC(*v, ld * sizeof(double));
   if (s->smith) SYS_ALLOC(s->phase, phase_scratch_bytes(s->N, s->tables, s->prec));
   SYS_ALLOC(s->chol_work, cholesky_work_bytes(s->ld, s->prec));
@@ -250,6 +305,19 @@ int compute_Dff(pbg_system* s, cudaStream_t st) {
     return launch_pad_identity(s->D, s->n, s->ld, s->prec, st);
   }
   const double scale = 1e19 / p.viscosity;
+  if (s->mlub) {
+    // Mff in FP32, Rff = inv(Mff) on the tensor cores (a copy is factored)
+    rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, PBG_PREC_MIXED, s->Mff, s->ld, s->phase,
+                           st);
+    if (rc) return rc;
+    rc = launch_pad_identity(s->Mff, s->n, s->ld, PBG_PREC_MIXED, st);
+    if (rc) return rc;
+    const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
+    PBG_CUDA_TRY(cudaMemcpyAsync(w.F, s->Mff, (size_t)s->ld * s->ld * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    s->work_holds_R = false;
+    if ((rc = tc_factor_invert(s->ld, s->dflags + 2, s->inv_work, st))) return rc;
+    return tc_lauum(w.X, s->ld, 1.0f, false, (float*)s->Rff, st);
+  }
   rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, PBG_PREC_FP64, s->Mff, s->ld, s->phase, st);
   if (rc) return rc;
   rc = launch_pad_identity(s->Mff, s->n, s->ld, PBG_PREC_FP64, st);
@@ -258,9 +326,32 @@ int compute_Dff(pbg_system* s, cudaStream_t st) {
   return launch_spd_inverse(s->Rff, s->n, s->ld, s->dflags + 2, s->inv_work, st);
 }
 
+// Mixed lubricated path: G = chol(J R J) and X = inv(G) on the tensor cores
+// (FP64 diagonal tiles, 3xTF32 trailing updates); then inv(R) = J X^T X J.
+static int factor_reversed_R(pbg_system* s, int* info, cudaStream_t st) {
+  const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
+  const long long total = (long long)s->ld * s->ld;
+  reverse_narrow_kernel<<<grid_for(total), 256, 0, st>>>(s->R, s->ld, w.F);
+  PBG_CHECK_LAUNCH();
+  int rc = tc_factor_invert(s->ld, info, s->inv_work, st);
+  s->work_holds_R = rc == PBG_OK;
+  return rc;
+}
+
 // box.py:533-541: R = C eta / 1e19 + Rff ; D = kBT inv(R).
 int compute_Dtot(pbg_system* s, cudaStream_t st) {
   const pbg_params& p = s->p;
+  if (s->mlub) {
+    const long long total = (long long)s->ld * s->ld;
+    widen_matrix_kernel<<<grid_for(total), 256, 0, st>>>((const float*)s->Rff, s->R, total);
+    PBG_CHECK_LAUNCH();
+    int rc = launch_lubrication_add(pair_source(s), s->radii, p.lubrication_cutoff, p.cichocki_correction,
+                                    p.viscosity / 1e19, s->R, s->ld, st);
+    if (rc) return rc;
+    if ((rc = factor_reversed_R(s, s->dflags + 3, st))) return rc;
+    const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
+    return tc_lauum(w.X, s->ld, (float)p.kBT, true, (float*)s->D, st);
+  }
   const size_t bytes = (size_t)s->ld * s->ld * sizeof(double);
   PBG_CUDA_TRY(cudaMemcpyAsync(s->R, s->Rff, bytes, cudaMemcpyDeviceToDevice, st));
   int rc = launch_lubrication_add(pair_source(s), s->radii, p.lubrication_cutoff, p.cichocki_correction,
@@ -277,6 +368,20 @@ int compute_Dtot(pbg_system* s, cudaStream_t st) {
 // box.py:546-556: B = chol(D), lower.
 int decompose(pbg_system* s, cudaStream_t st) {
   if (s->p.hydrodynamics == PBG_HI_NONE) return PBG_OK;
+  if (s->mlub) {
+    // chol(kBT inv(R)) = sqrt(kBT) J G^{-T} J: read off X = inv(G), no second factorisation
+    int rc;
+    if (!s->work_holds_R && (rc = factor_reversed_R(s, s->dflags + 1, st))) return rc;
+    const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
+    if ((rc = tc_reversed_factor(w.X, w.F, s->ld, std::sqrt(s->p.kBT), (float*)s->B, (float*)s->chol_work, st)))
+      return rc;
+    // keep G and its diagonal inverses: the noise products use them directly
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->G, w.F, (size_t)s->ld * s->ld * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    PBG_CUDA_TRY(cudaMemcpyAsync(s->Ginv, w.invdiag, (size_t)PBG_TILE * s->ld * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, st));
+    s->g_valid = true;
+    return PBG_OK;
+  }
   const long long total = (long long)s->ld * s->ld;
   if (s->prec == PBG_PREC_FP64)
     copy_lower_pad_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)s->D, (double*)s->B, s->n, s->ld);
@@ -298,8 +403,32 @@ static int overlap_check(pbg_system* s, cudaStream_t st, bool* overlap) {
   return PBG_OK;
 }
 
+// Mixed lubricated path: x = R^{-1} b from the FP32 D = kBT inv(R) with one
+// step of iterative refinement against the FP64 R:
+//   x0 = D b / kBT,  x = x0 + D (b - R x0) / kBT  (residual in FP64).
+static int refined_solve(pbg_system* s, const void* D, const double* R, const double* b, double* x,
+                         cudaStream_t st) {
+  const int n = s->n;
+  const double c = 1.0 / s->p.kBT;
+  int rc = launch_gemv_scaled(D, s->ld, n, s->prec, b, c, x, st);
+  if (rc) return rc;
+  residual_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(R, s->ld, n, b, x, s->res);
+  PBG_CHECK_LAUNCH();
+  if ((rc = launch_gemv_scaled(D, s->ld, n, s->prec, s->res, c, s->corr, st))) return rc;
+  add_vec_kernel<<<(n + 255) / 256, 256, 0, st>>>(x, s->corr, n);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
 // Deterministic step (box.py:353-362): pos += ((dt/kBT) D @ F) * mult.
 static int deterministic_step(pbg_system* s, const void* D, double mult, cudaStream_t st) {
+  if (s->mlub) {
+    // (dt/kBT) D F = dt R^{-1} F, by the refined solve
+    int rc = refined_solve(s, D, s->R, step_force(s), s->sol, st);
+    if (rc) return rc;
+    if ((rc = launch_scale2(s->sol, s->dt, mult, s->n, s->FX, st))) return rc;
+    return launch_translate(s->pos, s->FX, s->n, false, st);
+  }
   int rc = launch_gemv_scaled(D, s->ld, s->n, s->prec, step_force(s), s->dt / s->p.kBT, s->FX, st);
   if (rc) return rc;
   rc = launch_scale2(s->FX, 1.0, mult, s->n, s->FX, st);
@@ -343,6 +472,10 @@ __global__ void div_apply_kernel(double* __restrict__ div, int n, double eps, do
 }
 
 int set_divergence(pbg_system* s, bool on) {
+  if (on && s->mlub) {
+    pbg_set_error_message("the divergence term needs precision fp64 in the lubrication modes");
+    return PBG_ERR_ARG;
+  }
   if (on && !s->div) {
     const size_t mat = (size_t)s->ld * s->ld;
     bool ok = cudaMalloc(&s->div, s->ld * sizeof(double)) == cudaSuccess;
@@ -427,6 +560,7 @@ int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol,
 static int midpoint_rebuild(pbg_system* s, cudaStream_t st) {
   const size_t bytes = (size_t)s->ld * s->ld * s->es;
   const size_t bytes64 = (size_t)s->ld * s->ld * sizeof(double);
+  const size_t bytes_ff = s->mlub ? (size_t)s->ld * s->ld * sizeof(float) : bytes64;
   std::swap(s->D, s->D0);
   if (s->lub) {
     std::swap(s->Mff, s->Mff0);
@@ -443,8 +577,8 @@ static int midpoint_rebuild(pbg_system* s, cudaStream_t st) {
   } else {
     PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->D0, bytes, cudaMemcpyDeviceToDevice, st));
     if (s->lub) {
-      PBG_CUDA_TRY(cudaMemcpyAsync(s->Mff, s->Mff0, bytes64, cudaMemcpyDeviceToDevice, st));
-      PBG_CUDA_TRY(cudaMemcpyAsync(s->Rff, s->Rff0, bytes64, cudaMemcpyDeviceToDevice, st));
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->Mff, s->Mff0, bytes_ff, cudaMemcpyDeviceToDevice, st));
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->Rff, s->Rff0, bytes_ff, cudaMemcpyDeviceToDevice, st));
     }
   }
   if (s->lub) {
@@ -462,12 +596,32 @@ static int midpoint_rebuild(pbg_system* s, cudaStream_t st) {
 }
 
 static void midpoint_restore(pbg_system* s) {
+  s->work_holds_R = false;  // the workspace holds the midpoint R's factor
   std::swap(s->D, s->D0);
   if (s->lub) {
     std::swap(s->Mff, s->Mff0);
     std::swap(s->Rff, s->Rff0);
     std::swap(s->R, s->R0);
   }
+}
+
+// Mixed lubricated path, from the FP32 factor G of J R0 J (backward-stable
+// triangular solve and product instead of the explicit FP32 B):
+//   U = B0 xi = sqrt(kBT) J G^{-T} J xi,   y = inv(B0^T) xi = J G J xi / sqrt(kBT).
+static int noise_from_G(pbg_system* s, cudaStream_t st) {
+  const int ld = s->ld, g = (ld + 255) / 256;
+  const double sk = std::sqrt(s->p.kBT);
+  reverse_scale_kernel<<<g, 256, 0, st>>>(s->xi, ld, 1.0, s->res);
+  PBG_CHECK_LAUNCH();
+  int rc = launch_trsv_upper(s->G, ld, PBG_PREC_MIXED, s->Ginv, s->res, s->rwork, s->corr, st);
+  if (rc) return rc;
+  reverse_scale_kernel<<<g, 256, 0, st>>>(s->corr, ld, sk, s->U);
+  PBG_CHECK_LAUNCH();
+  if (s->p.propagation_scheme != PBG_SCHEME_MIDPOINT) return PBG_OK;
+  if ((rc = launch_trmv_lower(s->G, ld, ld, PBG_PREC_MIXED, s->res, s->corr, st))) return rc;
+  reverse_scale_kernel<<<g, 256, 0, st>>>(s->corr, ld, 1.0 / sk, s->y);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
 }
 
 int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st) {
@@ -479,7 +633,12 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
   const int n = s->n;
   int rc;
   PBG_CUDA_TRY(cudaMemcpyAsync(s->xi, xi, n * sizeof(double), cudaMemcpyDefault, st));
-  if ((rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st))) return rc;
+  const bool from_G = s->mlub && s->g_valid;
+  if (from_G) {
+    if ((rc = noise_from_G(s, st))) return rc;
+  } else if ((rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st))) {
+    return rc;
+  }
   bool overlap = false;
   if (s->p.propagation_scheme == PBG_SCHEME_ERMAK) {
     // box.py:219-248
@@ -503,14 +662,34 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
     return PBG_OK;
   }
   if ((rc = midpoint_rebuild(s, st))) return rc;
-  // deterministic drift m dt / (2 kBT) (D' - D0) @ F
-  if ((rc = launch_gemv_diff(s->D, s->D0, s->ld, n, s->prec, step_force(s), m * s->dt / (2 * s->p.kBT), s->ddet,
-                             st)))
+  // deterministic drift m dt / (2 kBT) (D' - D0) @ F; in the mixed lubricated
+  // path (m dt / 2) (R'^{-1} F - R0^{-1} F) by refined solves
+  if (s->mlub) {
+    if ((rc = refined_solve(s, s->D, s->R, step_force(s), s->sol, st))) return rc;
+    if ((rc = refined_solve(s, s->D0, s->R0, step_force(s), s->sol0, st))) return rc;
+    diff_scaled_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->sol, s->sol0, m * s->dt / 2, n, s->ddet);
+    PBG_CHECK_LAUNCH();
+  } else if ((rc = launch_gemv_diff(s->D, s->D0, s->ld, n, s->prec, step_force(s), m * s->dt / (2 * s->p.kBT),
+                                    s->ddet, st))) {
     return rc;
+  }
   // stochastic drift m/2 sqrt(2 dt) (D' inv(B0^T) - B0) @ xi = c2 (D' y - B0 xi), B0^T y = xi
-  if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) return rc;
-  if ((rc = launch_gemv_scaled(s->D, s->ld, n, s->prec, s->y, 1.0, s->Dy, st))) return rc;
-  if ((rc = launch_drift_combine(s->Dy, s->U, s->ddet, m / 2 * std::sqrt(2 * s->dt), n, s->drift, st))) return rc;
+  if (!from_G && (rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) return rc;
+  if (s->mlub) {
+    // B0 xi = D0 y, so the drift is c2 kBT (R'^{-1} y - R0^{-1} y): both terms
+    // by refined solves, so that the FP32 rounding of B0 does not enter the
+    // difference (c2 = 50 sqrt(2 dt) at m = 100 amplifies any mismatch)
+    if ((rc = refined_solve(s, s->D, s->R, s->y, s->sol, st))) return rc;
+    if ((rc = refined_solve(s, s->D0, s->R0, s->y, s->sol0, st))) return rc;
+    const double c2 = m / 2 * std::sqrt(2 * s->dt);
+    diff_scaled_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->sol, s->sol0, c2 * s->p.kBT, n, s->drift);
+    PBG_CHECK_LAUNCH();
+    add_vec_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->drift, s->ddet, n);
+    PBG_CHECK_LAUNCH();
+  } else {
+    if ((rc = launch_gemv_scaled(s->D, s->ld, n, s->prec, s->y, 1.0, s->Dy, st))) return rc;
+    if ((rc = launch_drift_combine(s->Dy, s->U, s->ddet, m / 2 * std::sqrt(2 * s->dt), n, s->drift, st))) return rc;
+  }
   midpoint_restore(s);
   if ((rc = deterministic_step(s, s->D, 1.0 - 1.0 / m, st))) return rc;
   if ((rc = stochastic_step(s, 1.0 - 1.0 / m, st))) return rc;
@@ -641,8 +820,8 @@ int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t s
   switch (which) {
     case PBG_MAT_D: dst = s->D; prec = s->prec; break;
     case PBG_MAT_B: dst = s->B; prec = s->prec; break;
-    case PBG_MAT_MFF: dst = s->Mff; break;
-    case PBG_MAT_RFF: dst = s->Rff; break;
+    case PBG_MAT_MFF: dst = s->Mff; prec = s->mlub ? PBG_PREC_MIXED : PBG_PREC_FP64; break;
+    case PBG_MAT_RFF: dst = s->Rff; prec = s->mlub ? PBG_PREC_MIXED : PBG_PREC_FP64; break;
     case PBG_MAT_R: dst = s->R; break;
     default: return PBG_ERR_ARG;
   }
@@ -669,6 +848,8 @@ int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t s
     PBG_CUDA_TRY(cudaStreamSynchronize(st));
     PBG_CUDA_TRY(cudaFreeAsync(stage, st));
   }
+  if (which == PBG_MAT_R) s->work_holds_R = false;
+  if (which == PBG_MAT_B) s->g_valid = false;  // the noise then comes from the explicit B
   return rc;
 }
 
@@ -678,8 +859,8 @@ int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st) {
   switch (which) {
     case PBG_MAT_D: src = s->D; prec = s->prec; break;
     case PBG_MAT_B: src = s->B; prec = s->prec; lower = 1; break;
-    case PBG_MAT_MFF: src = s->Mff; break;
-    case PBG_MAT_RFF: src = s->Rff; break;
+    case PBG_MAT_MFF: src = s->Mff; prec = s->mlub ? PBG_PREC_MIXED : PBG_PREC_FP64; break;
+    case PBG_MAT_RFF: src = s->Rff; prec = s->mlub ? PBG_PREC_MIXED : PBG_PREC_FP64; break;
     case PBG_MAT_R: src = s->R; break;
     default: return PBG_ERR_ARG;
   }

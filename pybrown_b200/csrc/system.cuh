@@ -14,6 +14,13 @@ struct pbg_system {
   pbg_params p{};
   int N = 0, n = 0, ld = 0;  // beads, matrix order 3N, padded order
   bool lub = false, smith = false;
+  // Mixed lubricated path (lubrication modes, precision "mixed"): Mff, Rff
+  // (and their midpoint copies) are FP32, R stays FP64, D and B are FP32.
+  bool mlub = false;
+  bool work_holds_R = false;  // inv_work holds G = chol(J R J) and inv(G) of the current R
+  void* G = nullptr;          // mlub: FP32 G of the step-start R (noise factor B = sqrt(kBT) J G^{-T} J)
+  void* Ginv = nullptr;       // mlub: inverted diagonal tiles of G
+  bool g_valid = false;       // G and Ginv belong to the B in use
   int prec = PBG_PREC_FP64;  // element type of D and B
   size_t es = 8;
   const pbg::EwaldTables* tables = nullptr;
@@ -26,13 +33,14 @@ struct pbg_system {
   void* D = nullptr;           // ld x ld, prec
   void* B = nullptr;           // ld x ld, prec, lower factor
   void* D0 = nullptr;          // midpoint: step-start D
-  double *Mff = nullptr, *Rff = nullptr, *R = nullptr;     // lubrication modes
+  double *Mff = nullptr, *Rff = nullptr, *R = nullptr;     // lubrication modes (Mff, Rff FP32 if mlub)
   double *Mff0 = nullptr, *Rff0 = nullptr, *R0 = nullptr;  // midpoint copies
   double *FX = nullptr, *U = nullptr, *BX = nullptr, *ddet = nullptr, *y = nullptr;
   double *rwork = nullptr, *Dy = nullptr, *drift = nullptr, *xi = nullptr;  // ld each
+  double *sol = nullptr, *sol0 = nullptr, *res = nullptr, *corr = nullptr;  // ld each: refined solves (mlub)
   void* phase = nullptr;       // Ewald phase tables
   void* chol_work = nullptr;   // inverted diagonal tiles of B
-  void* inv_work = nullptr;    // SPD inverse workspace
+  void* inv_work = nullptr;    // SPD inverse workspace (tensor-core inverse workspace if mlub)
   int* dflags = nullptr;       // [0] overlap, [1] cholesky info, [2] Rff info, [3] D info
   bool divergence = false;     // divergence term of the lubricated D (Ermak scheme)
   double* div = nullptr;       // ld: its value this step

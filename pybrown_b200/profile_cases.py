@@ -3,11 +3,13 @@
     python -m pybrown_b200.profile_cases cholesky --order 768 --precision mixed
     python -m pybrown_b200.profile_cases smith --beads 512 --precision fp64
     python -m pybrown_b200.profile_cases batch --replicas 64 --precision mixed
+    python -m pybrown_b200.profile_cases lub --beads 512 --precision fp64
 
 `cholesky` factors the Smith-Ewald diffusion matrix of a random bead
 configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it;
 `batch` advances a batch of replicas (N uniform in [32, 512], seed 1) by one
-step.
+step; `lub` takes one midpoint step of a lubricated box (rpy_smith_lub,
+radius 20, volume fraction 0.30, cutoff 0.5, Cichocki, m = 100, dt 0.1).
 Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
 time of one launch.
 """
@@ -17,7 +19,7 @@ import math
 import numpy as np
 
 
-def _config(seed, n, L, a_lo=10.0, a_hi=40.0):
+def _config(seed, n, L, a_lo=10.0, a_hi=40.0, gap=0.0):
     rng = np.random.default_rng(seed)
     pos = np.zeros((n, 3))
     radii = np.zeros(n)
@@ -28,7 +30,7 @@ def _config(seed, n, L, a_lo=10.0, a_hi=40.0):
         if k:
             d = pos[:k] - p
             d -= L * np.round(d / L)
-            if np.any(np.sqrt((d * d).sum(1)) <= radii[:k] + a):
+            if np.any(np.sqrt((d * d).sum(1)) <= radii[:k] + a + gap):
                 continue
         pos[k], radii[k] = p, a
         k += 1
@@ -40,7 +42,7 @@ def main(argv=None):
 
     from . import _lib
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("kernel", choices=("cholesky", "smith", "batch"))
+    ap.add_argument("kernel", choices=("cholesky", "smith", "batch", "lub"))
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--beads", type=int, default=256)
     ap.add_argument("--order", type=int, default=0, help="cholesky: matrix order (default 3 x beads)")
@@ -49,6 +51,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return _batch(a, torch)
+    if a.kernel == "lub":
+        return _lub(a, torch)
     prec = _lib.PREC[a.precision]
     dtype = torch.float64 if prec == 0 else torch.float32
     beads = a.order // 3 if a.order else a.beads
@@ -111,6 +115,33 @@ def _batch(a, torch):
         total += start.elapsed_time(end)
     print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}): {total / a.reps:.3f} ms per step")
     batch.close()
+
+
+def _lub(a, torch):
+    from .bead import Bead
+    from .box import Box
+    N, radius, phi = a.beads, 20.0, 0.30
+    L = (N * 4.0 * math.pi * radius ** 3 / 3.0 / phi) ** (1.0 / 3.0)
+    pos, radii = _config(0, N, L, radius, radius, gap=0.05 * radius)
+    inp = {"box_length": L, "T": 293.15, "viscosity": 0.01005, "seed": 0, "hydrodynamics": "rpy_smith_lub",
+           "ewald_alpha": math.sqrt(math.pi), "ewald_real": 2, "ewald_imag": 4, "lubrication_cutoff": 0.5,
+           "cichocki_correction": True, "propagation_scheme": "midpoint", "m_midpoint": 100.0,
+           "immobile_labels": [], "check_overlaps": True, "overlap_treshold": 0.0, "max_move_attempts": 1000000,
+           "external_force": [0.0, 0.0, 0.0], "energy_unit": "joule", "verbose": False, "debug": False,
+           "precision": a.precision, "lennard_jones_6": False, "lennard_jones_12": False,
+           "custom_interactions": False}
+    box = Box([Bead(p, r) for p, r in zip(pos, radii)], inp)
+    box.propagate(0.1)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(a.reps):
+        start.record()
+        box.propagate(0.1)
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    print(f"lub N={N} L={L:.1f} ({a.precision}): {total / a.reps:.3f} ms per step")
 
 
 if __name__ == "__main__":

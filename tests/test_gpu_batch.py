@@ -184,6 +184,40 @@ def test_alone_equals_mix_with_changing_membership():
     assert np.all(np.isfinite(alone)) and not np.array_equal(alone[0], alone[-1])
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_autotuned_schedule_changes_no_result(precision):
+    """The schedule autotuner (merge order of the replicas' task segments x
+    CTAs per SM) times every candidate on the current matrices and keeps the
+    fastest; trajectories with the tuned schedule, and with each fixed
+    schedule, are bit-identical to the default one."""
+    from pybrown_b200.batch import ReplicaBatch
+    configs = [_config(500 + k, N, 0.05, 10.0, 30.0) for k, N in enumerate((40, 130, 75, 200, 33))]
+
+    def run(schedule):
+        batch = ReplicaBatch(precision=precision)
+        slots = [batch.add(p, r, l, seed=70 + k, noise="device") for k, (p, r, l) in enumerate(configs)]
+        tuned = None
+        out = []
+        for step in range(5):
+            if step == 1 and schedule == "auto":
+                tuned = batch.autotune(reps=1)
+            elif step == 1 and schedule is not None:
+                batch.set_schedule(*schedule)
+            batch.propagate(1.0)
+            out.append(np.concatenate([batch.positions(s).ravel() for s in slots]))
+        batch.close()
+        return np.array(out), tuned
+
+    ref, _ = run(None)
+    got, tuned = run("auto")
+    assert np.array_equal(ref, got)
+    n_cand = 8 if precision == "mixed" else 4
+    assert len(tuned["ms"]) == n_cand and all(v > 0 for v in tuned["ms"].values())
+    assert tuned["ms"][(tuned["merge_order"], tuned["ctas_per_sm"])] == min(tuned["ms"].values())
+    for sched in (("replica_major", 1), ("smaller_first", 0), ("added", 1)):
+        assert np.array_equal(ref, run(sched)[0]), sched
+
+
 def test_device_noise_is_standard_normal():
     """The counter-based stream has mean 0, variance 1 and no correlation
     between neighbouring draws, seen through the moves of a very dilute rpy

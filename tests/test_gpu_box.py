@@ -136,3 +136,41 @@ def test_box_pickle_resume_bit_exact():
     for _ in range(3):
         resumed.propagate(1.0)
     assert all(np.array_equal(o, r.r) for o, r in zip(original, resumed.beads))
+
+
+# Bars of the mixed lubricated path (max-abs / max against the FP64 oracle).
+# The FP32 far-field inverse sets them: cond(Mff) ~ 2e2 and cond(R) ~ 7e2 at
+# phi = 0.3 turn FP32 rounding into ~1e-5 in Rff, D and B; the midpoint drift
+# multiplies the difference of two solves by m/2 = 50.
+MLUB_BARS = {"ermak": 5e-5, "midpoint": 5e-4}
+
+
+@pytest.mark.parametrize("scheme", ["midpoint", "ermak"])
+def test_box_mixed_lubrication(oracle_lib, scheme):
+    """Mixed lubricated path (FP32 far-field mobility and its tensor-core
+    inverse, FP64 near-field correction and R, the FP32 factor of the
+    reversed R for the noise, FP64-refined solves for D F and the midpoint
+    drift) against the FP64 oracle at a dense packing (phi 0.3, gap >= 0.05 a),
+    with the rebuild flags of diff_freq / lub_freq / chol_freq exercised on
+    the Ermak run."""
+    from oracle.oracle import OracleBox
+    N, a = 128, 20.0
+    L = (N * 4 * math.pi * a ** 3 / 3 / 0.30) ** (1 / 3)
+    pos, radii = _config(7, N, L, a, a, 0.05 * a)
+    inp = _inp(box_length=L, hydrodynamics="rpy_smith_lub", propagation_scheme=scheme, lubrication_cutoff=0.5)
+    box = _box(pos, radii, dict(inp, precision="mixed"))
+    ref = OracleBox(pos, radii, inp, clib=oracle_lib)
+    flags = [(True, True, True)] * 6
+    if scheme == "ermak":
+        flags = [(True, True, True), (False, True, True), (True, True, False), (False, False, True),
+                 (True, True, True), (False, True, False)]
+    for b_ff, b_nf, chol in flags:
+        box.propagate(0.1, build_Dff=b_ff, build_Dnf=b_nf, cholesky=chol)
+        ref.propagate(0.1, build_Dff=b_ff, build_Dnf=b_nf, cholesky=chol)
+        assert box.draw_count == ref.draw_count
+    got = np.array([b.r for b in box.beads])
+    assert rel_err(got - pos, ref.pos - pos) <= MLUB_BARS[scheme]
+    assert rel_err(box.R, ref.R) <= 1e-5
+    assert rel_err(box.Rff, ref.Rff) <= 5e-5
+    assert rel_err(box.D, ref.D) <= 1e-4
+    assert rel_err(box.B, ref.B) <= 1e-4
