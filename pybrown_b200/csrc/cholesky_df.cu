@@ -47,6 +47,7 @@ namespace {
 
 constexpr int NB = 64;
 constexpr int THREADS = 256;
+constexpr int TILE_PER_THREAD = 64 * 64 / THREADS;  // elements of a 64 x 64 tile per thread
 constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
@@ -1022,9 +1023,16 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
       double* Tm = Xw + NB * LDA;
       double* Rv = Tm + 32 * 36;
       const T* g = tile<T>(a, k, k);
-      for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
-        const int r = e >> 6, c = e & 63;
-        Lk[r * LDA + c] = c <= r ? (double)ldcg(g + (size_t)r * a.ld + c) : 0.0;
+      T v[TILE_PER_THREAD];  // all loads in flight before the first store
+#pragma unroll
+      for (int q = 0; q < TILE_PER_THREAD; ++q) {
+        const int e = threadIdx.x + q * THREADS;
+        v[q] = ldcg(g + (size_t)(e >> 6) * a.ld + (e & 63));
+      }
+#pragma unroll
+      for (int q = 0; q < TILE_PER_THREAD; ++q) {
+        const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
+        Lk[r * LDA + c] = c <= r ? (double)v[q] : 0.0;
       }
       __syncthreads();
       if (threadIdx.x < NB) Rv[threadIdx.x] = 1.0 / Lk[threadIdx.x * LDA + threadIdx.x];
@@ -1471,22 +1479,43 @@ constexpr size_t tc_smem_bytes() {
   return 2 * NB * LDA * sizeof(T);
 }
 
-// s[c][r] = g[r][c] for a 64 x 64 tile (rows of LDA in smem).
+// Transposed staging of a 64 x 64 tile, s[c][r] = g[r][c] (rows of LDA in
+// smem), in two halves so that a thread's 16 global loads are all in flight
+// before the first shared store: load_tile_regs, then store_tile_transposed.
+template <typename T>
+__device__ __forceinline__ void load_tile_regs(const T* __restrict__ g, int ld, T (&v)[TILE_PER_THREAD]) {
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) {
+    const int e = threadIdx.x + q * THREADS;
+    v[q] = g[(size_t)(e >> 6) * ld + (e & 63)];
+  }
+}
+template <typename T>
+__device__ __forceinline__ void store_tile_transposed(const T (&v)[TILE_PER_THREAD], T* s) {
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) {
+    const int e = threadIdx.x + q * THREADS;
+    s[(e & 63) * LDA + (e >> 6)] = v[q];
+  }
+}
 template <typename T>
 __device__ __forceinline__ void stage_transposed(const T* __restrict__ g, int ld, T* s) {
-  for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
-    const int r = e >> 6, c = e & 63;
-    s[c * LDA + r] = g[(size_t)r * ld + c];
-  }
+  T v[TILE_PER_THREAD];
+  load_tile_regs(g, ld, v);
+  store_tile_transposed(v, s);
 }
 
 // inv(L_kk) with its upper triangle zeroed, into smem rows of LDA.
 template <typename T>
 __device__ __forceinline__ void stage_invdiag(const T* __restrict__ invdiag, int k, T* s) {
   const T* inv = invdiag + (size_t)k * NB * NB;
-  for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
-    const int r = e >> 6, c = e & 63;
-    s[r * LDA + c] = c <= r ? inv[e] : T(0);
+  T v[TILE_PER_THREAD];
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) v[q] = inv[threadIdx.x + q * THREADS];
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) {
+    const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
+    s[r * LDA + c] = c <= r ? v[q] : T(0);
   }
 }
 
@@ -1506,9 +1535,13 @@ __global__ void __launch_bounds__(THREADS) trsm_step_kernel(const T* __restrict_
   if ((int)blockIdx.x == nupd) {
     T* g = X + (size_t)(k + 1) * NB * ld + (size_t)(k + 1) * NB;
     const T* inv = invdiag + (size_t)(k + 1) * NB * NB;
-    for (int e = threadIdx.x; e < NB * NB; e += THREADS) {
-      const int r = e >> 6, c = e & 63;
-      g[(size_t)r * ld + c] = c <= r ? inv[e] : T(0);
+    T v[TILE_PER_THREAD];
+#pragma unroll
+    for (int q = 0; q < TILE_PER_THREAD; ++q) v[q] = inv[threadIdx.x + q * THREADS];
+#pragma unroll
+    for (int q = 0; q < TILE_PER_THREAD; ++q) {
+      const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
+      g[(size_t)r * ld + c] = c <= r ? v[q] : T(0);
     }
     return;
   }
@@ -1555,10 +1588,18 @@ __global__ void __launch_bounds__(THREADS) lauum_tc_kernel(const T* __restrict__
   T acc[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  // the tiles of step k+1 are loaded into registers while step k multiplies
+  T va[TILE_PER_THREAD], vb[TILE_PER_THREAD];
+  load_tile_regs(X + (size_t)I * NB * ld + (size_t)I * NB, ld, va);
+  load_tile_regs(X + (size_t)I * NB * ld + (size_t)J * NB, ld, vb);
   for (int k = I; k < nt; ++k) {
-    stage_transposed(X + (size_t)k * NB * ld + (size_t)I * NB, ld, sA);
-    stage_transposed(X + (size_t)k * NB * ld + (size_t)J * NB, ld, sB);
+    store_tile_transposed(va, sA);
+    store_tile_transposed(vb, sB);
     __syncthreads();
+    if (k + 1 < nt) {
+      load_tile_regs(X + (size_t)(k + 1) * NB * ld + (size_t)I * NB, ld, va);
+      load_tile_regs(X + (size_t)(k + 1) * NB * ld + (size_t)J * NB, ld, vb);
+    }
     TileMMA<T>::sub(sA, sB, acc);
     __syncthreads();
   }
