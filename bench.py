@@ -444,6 +444,7 @@ def run_batch_section(args, torch):
     torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     launches = (_lib.lib.pbg_launch_count() - launches0) / args.steps
+    graph = batch.graph_state()
     beads = int(Ns.sum())
     batch.close()
     return {"workload": "256 replicas, N~U[32,512] (seed 1), a~U[10,30], phi=0.05, Smith-Ewald m=2 n=4, "
@@ -451,6 +452,7 @@ def run_batch_section(args, torch):
             "steps": args.steps, "ms_per_step": ms / args.steps,
             "bead_steps_per_s": beads * args.steps / (ms * 1e-3),
             "replica_steps_per_s": 256 * args.steps / (ms * 1e-3), "gpu_launches_per_step": launches,
+            "step_start_graph": {1: "one CUDA graph launch", 0: "direct launches", -1: "capture refused"}[graph],
             "schedule": {"merge_order": tune["merge_order"], "ctas_per_sm": tune["ctas_per_sm"],
                          "factorisation_ms": {f"{o}/{c}": round(v, 4) for (o, c), v in tune["ms"].items()}}}
 

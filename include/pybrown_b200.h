@@ -354,6 +354,12 @@ PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_s
  * best[2] = {merge_order, ctas_per_sm}; ms (may be NULL) receives the mean
  * time of each candidate, merge order major (8 entries). */
 PBG_API int pbg_batch_autotune(pbg_batch *b, int reps, int *best, float *ms, void *stream);
+/* How the start of a step (Ewald build, copy into B, factorisation,
+ * deterministic move) runs: 1 = one CUDA graph launch (captured once a step
+ * repeats with the same membership, flags and dt), 0 = its kernels launched
+ * one by one, -1 = the driver refused the capture (kernels launched one by
+ * one from then on).  No counterpart in the reference. */
+PBG_API int pbg_batch_graph_state(pbg_batch *b);
 
 #ifdef __cplusplus
 }

@@ -150,6 +150,7 @@ _SIGNATURES = {
     "pbg_batch_get_matrix": (_i, [_vp, _i, _i, _vp]),
     "pbg_batch_set_schedule": (_i, [_vp, _i, _i]),
     "pbg_batch_autotune": (_i, [_vp, _i, _ip, ctypes.POINTER(ctypes.c_float), _vp]),
+    "pbg_batch_graph_state": (_i, [_vp]),
     "pbg_selftest_wait_expiry": (_i, [_ll, _ip, ctypes.POINTER(ctypes.c_uint)]),
 }
 

@@ -146,6 +146,13 @@ class ReplicaBatch:
         table = {(self.MERGE_ORDERS[k // 2], k % 2 + 1): float(ms[k]) for k in range(8) if ms[k] >= 0}
         return {"merge_order": self.MERGE_ORDERS[best[0]], "ctas_per_sm": int(best[1]), "ms": table}
 
+    def graph_state(self):
+        """1 while the start of a step (Ewald build, factorisation,
+        deterministic move) replays one CUDA graph, 0 while its kernels are
+        launched one by one (the first step after a membership or flag
+        change), -1 if the driver refused the capture."""
+        return int(_lib.lib.pbg_batch_graph_state(self._h))
+
     # ---------------------------------------------------------------- step
     def propagate(self, dt, build_D=True, cholesky=True):
         """One step of every replica (box.py:150-250, Ermak scheme)."""

@@ -127,6 +127,16 @@ struct pbg_batch {
   int merge_order = PBG_MERGE_LARGER_FIRST;
   int ctas_per_sm = 0;
   bool have_D = false;  // a step has built D (the autotuner factors it)
+  // CUDA graph of the deterministic part of a step (Ewald build, copy into
+  // B, the persistent factorisation, the deterministic move), captured once a
+  // step repeats with the same membership and flags, replayed afterwards.
+  cudaStream_t cap_stream = nullptr;   // private non-blocking stream for the capture
+  cudaGraphExec_t begin_exec = nullptr;
+  long long begin_kernels = 0;         // kernel launches inside the graph
+  int key_build = -1, key_chol = -1, key_force = -1;
+  double key_dt = 0;
+  int key_repeats = 0;                 // steps in a row with the current key
+  bool graph_refused = false;          // the driver refused the capture: direct launches
 };
 
 namespace pbg {
@@ -354,6 +364,12 @@ __global__ void ewald_work_kernel(const int4* __restrict__ parts, int4* __restri
 // small per-replica descriptors from the host, the task and tile work lists
 // assembled on the device from each replica's cached list.
 int rebuild(pbg_batch* b, cudaStream_t st) {
+  if (b->begin_exec) {
+    cudaGraphExecDestroy(b->begin_exec);
+    b->begin_exec = nullptr;
+  }
+  b->key_repeats = 0;
+  b->key_build = -1;
   b->active.clear();
   for (int s = 0; s < (int)b->slots.size(); ++s)
     if (b->slots[s]) b->active.push_back(s);
@@ -572,6 +588,8 @@ PBG_API int pbg_batch_destroy(pbg_batch* b) {
   free_dev(b->d_stream);
   if (b->h_ovl) cudaFreeHost(b->h_ovl);
   if (b->h_info) cudaFreeHost(b->h_info);
+  if (b->begin_exec) cudaGraphExecDestroy(b->begin_exec);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   delete b;
   return PBG_OK;
 }
@@ -741,8 +759,67 @@ PBG_API int pbg_batch_fill_noise(pbg_batch* b, const unsigned char* mask, void* 
   return PBG_OK;
 }
 
+// The device work of a step's start: D (build_D), B = chol(D) (cholesky) of
+// every replica and the deterministic move of the replicas with a force.
+static int enqueue_begin(pbg_batch* b, double dt, int build_D, int cholesky, bool any_force, cudaStream_t st) {
+  const int R = (int)b->active.size();
+  const bool f64 = b->precision == PBG_PREC_FP64;
+  const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
+  int rc;
+  if (build_D && (rc = launch_rpy_batch(b->precision, smith, b->tables, b->d_rpy, b->d_ework, b->n_ework, R, st)))
+    return rc;
+  if (cholesky) {
+    const dim3 g(64, R);
+    if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
+    else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+    PBG_CHECK_LAUNCH();
+    PBG_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st));
+    if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, b->ctas_per_sm, st)))
+      return rc;
+  }
+  if (any_force) {
+    if (f64) batch_det_kernel<double><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
+    else batch_det_kernel<float><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
+    PBG_CHECK_LAUNCH();
+    batch_det_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps);
+    PBG_CHECK_LAUNCH();
+  }
+  return PBG_OK;
+}
+
+// Captures enqueue_begin into b->begin_exec on the private stream.  A refusal
+// by the driver (capture or instantiation) leaves graph_refused set and the
+// step runs its launches directly; any other error is returned.
+static int capture_begin(pbg_batch* b, double dt, int build_D, int cholesky, bool any_force) {
+  if (!b->cap_stream) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  const long long l0 = pbg_launch_count();
+  PBG_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeRelaxed));
+  int rc = enqueue_begin(b, dt, build_D, cholesky, any_force, b->cap_stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(b->cap_stream, &graph);
+  const long long kernels = pbg_launch_count() - l0;
+  pbg_count_launches(-kernels);  // nothing ran yet
+  if (rc != PBG_OK || end != cudaSuccess || !graph) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    b->graph_refused = true;
+    return PBG_OK;
+  }
+  const cudaError_t inst = cudaGraphInstantiate(&b->begin_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) {
+    cudaGetLastError();
+    b->begin_exec = nullptr;
+    b->graph_refused = true;
+    return PBG_OK;
+  }
+  b->begin_kernels = kernels;
+  return PBG_OK;
+}
+
 // Builds D (build_D) and B = chol(D) (cholesky) of every replica and applies
-// the deterministic step of the replicas with a force.
+// the deterministic step of the replicas with a force.  The second and later
+// steps with the same membership, flags and dt replay one CUDA graph.
 PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int cholesky, void* stream) {
   if (!b || !(dt > 0)) return PBG_ERR_ARG;
   if (b->in_step) {
@@ -758,37 +835,43 @@ PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int chole
     b->in_step = true;
     return PBG_OK;
   }
-  const bool f64 = b->precision == PBG_PREC_FP64;
-  const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
-  if (build_D && (rc = launch_rpy_batch(b->precision, smith, b->tables, b->d_rpy, b->d_ework, b->n_ework, R, st)))
-    return rc;
-  if (cholesky) {
-    const dim3 g(64, R);
-    if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
-    else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
-    PBG_CHECK_LAUNCH();
-    PBG_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st));
-    if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, b->ctas_per_sm, st)))
-      return rc;
-  }
-  if (build_D) b->have_D = true;
   bool any_force = false;
   for (int s : b->active) any_force = any_force || b->slots[s]->has_force;
-  if (any_force) {
-    if (f64) batch_det_kernel<double><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
-    else batch_det_kernel<float><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, dt);
-    PBG_CHECK_LAUNCH();
-    batch_det_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps);
-    PBG_CHECK_LAUNCH();
+  const bool same = b->key_build == build_D && b->key_chol == cholesky && b->key_force == (int)any_force &&
+                    b->key_dt == dt;
+  if (!same) {
+    if (b->begin_exec) {
+      cudaGraphExecDestroy(b->begin_exec);
+      b->begin_exec = nullptr;
+    }
+    b->key_build = build_D;
+    b->key_chol = cholesky;
+    b->key_force = (int)any_force;
+    b->key_dt = dt;
+    b->key_repeats = 0;
   }
+  ++b->key_repeats;
+  if (!b->begin_exec && !b->graph_refused && b->key_repeats >= 2 &&
+      (rc = capture_begin(b, dt, build_D, cholesky, any_force)))
+    return rc;
+  if (b->begin_exec) {
+    PBG_CUDA_TRY(cudaGraphLaunch(b->begin_exec, st));
+    pbg_count_launches(b->begin_kernels);
+  } else if ((rc = enqueue_begin(b, dt, build_D, cholesky, any_force, st))) {
+    return rc;
+  }
+  if (build_D) b->have_D = true;
   b->in_step = true;
   return PBG_OK;
 }
 
-// One stochastic attempt for the masked replicas (host array indexed by slot,
-// or null for all) with the noise already in place: U = B xi,
-// pos += U sqrt(2 dt), overlap test, undo on overlap.  accepted[slot] (host,
-// optional) is set to 1 or 0 for the masked replicas.
+// 1 while the start of a step replays a CUDA graph, 0 while it launches its
+// kernels directly, -1 if the driver refused the capture.
+PBG_API int pbg_batch_graph_state(pbg_batch* b) {
+  if (!b) return 0;
+  return b->graph_refused ? -1 : (b->begin_exec ? 1 : 0);
+}
+
 PBG_API int pbg_batch_step_attempt(pbg_batch* b, const unsigned char* mask, unsigned char* accepted, void* stream) {
   if (!b) return PBG_ERR_ARG;
   if (!b->in_step) {

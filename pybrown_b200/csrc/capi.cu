@@ -146,6 +146,7 @@ void pbg_record_cuda_error(cudaError_t e, const char* what, const char* file, in
 static std::atomic<long long> g_launches{0};
 
 void pbg_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void pbg_count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void pbg_set_error_message(const char* fmt, ...) {
   char buf[512];

@@ -1460,10 +1460,8 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
 
 // ---------------------------------------------------------------- SPD inverse on the tensor cores
 // inv(A) = X^T X with A = L L^T (the data-flow factorisation above) and
-// X = inv(L): X by a right-looking blocked solve of L X = I, one launch per
-// block row k (X_i. -= L_ik X_k. for every i > k, row k+1 finished with
-// inv(L_{k+1,k+1}) in the same launch) -- and X^T X with one CTA per lower
-// tile.  Every tile product is
+// X = inv(L): X level by level, joining pairs of finished diagonal blocks
+// (1 + 2 ceil(log2 nt) launches) -- and X^T X with one CTA per lower tile.  Every tile product is
 // TileMMA: FP64 DMMA for FP64 matrices, 3xTF32 split products with FP32
 // accumulation for FP32 ones.  Used by the SPD inverse of the FP64
 // lubrication path (cholesky.cu) and by the mixed lubricated path, which also
@@ -1505,9 +1503,36 @@ __device__ __forceinline__ void stage_transposed(const T* __restrict__ g, int ld
   store_tile_transposed(v, s);
 }
 
-// inv(L_kk) with its upper triangle zeroed, into smem rows of LDA.
+// inv(L) level by level (recursive doubling on the block structure): with
+// the diagonal tiles X_kk = inv(L_kk) in place, level s joins pairs of
+// finished diagonal blocks A = [2bs, 2bs+s) and C = [2bs+s, 2bs+2s) (tiles):
+//   inv([L_AA 0; L_CA L_CC]) = [X_AA 0; -X_CC L_CA X_AA, X_CC],
+// as two launches -- U = -L_CA X_AA, then X_CA = X_CC U -- so the whole
+// inverse takes 1 + 2 ceil(log2 nt) launches with no waits between CTAs.  U
+// lives in the (unused) upper triangle of X: U_ij at tile (a0+j, c0+i).
+
+// The tile of level s that CTA `idx` computes: pair (a0, c0), C row i, A
+// column j; false beyond the last tile.
+__device__ __forceinline__ bool level_tile(int nt, int s, int idx, int& a0, int& c0, int& i, int& j) {
+  for (int b = 0;; ++b) {
+    a0 = 2 * b * s;
+    c0 = a0 + s;
+    if (c0 >= nt) return false;
+    const int cnt = min(s, nt - c0) * s;
+    if (idx < cnt) {
+      i = idx / s;
+      j = idx % s;
+      return true;
+    }
+    idx -= cnt;
+  }
+}
+
+// X_kk = inv(L_kk), upper triangle zero (one CTA per diagonal tile).
 template <typename T>
-__device__ __forceinline__ void stage_invdiag(const T* __restrict__ invdiag, int k, T* s) {
+__global__ void __launch_bounds__(THREADS) trtri_diag_kernel(const T* __restrict__ invdiag, T* X, int ld) {
+  const int k = blockIdx.x;
+  T* g = X + (size_t)k * NB * ld + (size_t)k * NB;
   const T* inv = invdiag + (size_t)k * NB * NB;
   T v[TILE_PER_THREAD];
 #pragma unroll
@@ -1515,60 +1540,71 @@ __device__ __forceinline__ void stage_invdiag(const T* __restrict__ invdiag, int
 #pragma unroll
   for (int q = 0; q < TILE_PER_THREAD; ++q) {
     const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
-    s[r * LDA + c] = c <= r ? v[q] : T(0);
+    g[(size_t)r * ld + c] = c <= r ? v[q] : T(0);
   }
 }
 
-// Step k of the blocked solve L X = I (launched for k = -1 .. nt-2), with
-// block row k of X final on entry: CTA (i, c), i = k+1 .. nt-1, c = 0 .. k,
-// applies X_ic -= L_ik X_kc; the CTAs of row k+1 then finish that row,
-// X_{k+1,c} = inv(L_{k+1,k+1}) X_{k+1,c}, and the last CTA writes the
-// diagonal tile X_{k+1,k+1} = inv(L_{k+1,k+1}).  Rows > k+1 read only row k,
-// which nobody writes in this launch.
+// Level s, first half: U_ij = -sum_{k=j}^{s-1} L_{c0+i, a0+k} X_{a0+k, a0+j}
+// (X_AA lower), stored at tile (a0+j, c0+i).
 template <typename T>
-__global__ void __launch_bounds__(THREADS) trsm_step_kernel(const T* __restrict__ L, const T* __restrict__ invdiag,
-                                                            int k, T* X, int ld, int nt) {
+__global__ void __launch_bounds__(THREADS) trtri_level_u_kernel(const T* __restrict__ L, T* X, int ld, int nt,
+                                                                int s) {
   extern __shared__ __align__(16) unsigned char smem[];
   T* sA = reinterpret_cast<T*>(smem);
   T* sB = sA + NB * LDA;
-  const int nupd = (nt - k - 1) * (k + 1);
-  if ((int)blockIdx.x == nupd) {
-    T* g = X + (size_t)(k + 1) * NB * ld + (size_t)(k + 1) * NB;
-    const T* inv = invdiag + (size_t)(k + 1) * NB * NB;
-    T v[TILE_PER_THREAD];
-#pragma unroll
-    for (int q = 0; q < TILE_PER_THREAD; ++q) v[q] = inv[threadIdx.x + q * THREADS];
-#pragma unroll
-    for (int q = 0; q < TILE_PER_THREAD; ++q) {
-      const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
-      g[(size_t)r * ld + c] = c <= r ? v[q] : T(0);
-    }
-    return;
-  }
-  const int i = k + 1 + blockIdx.x / (k + 1), c = blockIdx.x % (k + 1);
-  stage_async(L + (size_t)i * NB * ld + (size_t)k * NB, ld, sA, LDA);
-  stage_transposed(X + (size_t)k * NB * ld + (size_t)c * NB, ld, sB);
-  T* Xic = X + (size_t)i * NB * ld + (size_t)c * NB;
+  int a0, c0, i, j;
+  if (!level_tile(nt, s, blockIdx.x, a0, c0, i, j)) return;
+  const int ci = c0 + i, aj = a0 + j;
   T acc[16];
-  load_acc(Xic, ld, acc);
-  cp_async_wait_all();
-  __syncthreads();
-  TileMMA<T>::sub(sA, sB, acc);
-  if (i == k + 1) {
-    __syncthreads();  // sA, sB free
 #pragma unroll
-    for (int rs = 0; rs < 2; ++rs)
-#pragma unroll
-      for (int cs = 0; cs < 8; ++cs) sB[acc_col(cs) * LDA + acc_row(rs)] = acc[TileMMA<T>::idx(rs, cs)];
-    stage_invdiag(invdiag, k + 1, sA);
+  for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  T vb[TILE_PER_THREAD];
+  load_tile_regs(X + (size_t)(a0 + j) * NB * ld + (size_t)aj * NB, ld, vb);
+  for (int k = j; k < s; ++k) {
+    stage_async(L + (size_t)ci * NB * ld + (size_t)(a0 + k) * NB, ld, sA, LDA);
+    store_tile_transposed(vb, sB);
+    if (k + 1 < s) load_tile_regs(X + (size_t)(a0 + k + 1) * NB * ld + (size_t)aj * NB, ld, vb);
+    cp_async_wait_all();
     __syncthreads();
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = T(0);
-    TileMMA<T>::sub(sA, sB, acc);  // acc = -inv(L_{k+1,k+1}) X_{k+1,c}
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
+    TileMMA<T>::sub(sA, sB, acc);
+    __syncthreads();
   }
-  store_acc(Xic, ld, acc);
+  store_acc(X + (size_t)aj * NB * ld + (size_t)ci * NB, ld, acc);
+}
+
+// Level s, second half: X_{c0+i, a0+j} = sum_{k=0}^{i} X_{c0+i, c0+k} U_kj.
+template <typename T>
+__global__ void __launch_bounds__(THREADS) trtri_level_x_kernel(T* X, int ld, int nt, int s) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* sA = reinterpret_cast<T*>(smem);
+  T* sB = sA + NB * LDA;
+  int a0, c0, i, j;
+  if (!level_tile(nt, s, blockIdx.x, a0, c0, i, j)) return;
+  const int ci = c0 + i, aj = a0 + j;
+  T acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  T vb[TILE_PER_THREAD];
+  load_tile_regs(X + (size_t)aj * NB * ld + (size_t)c0 * NB, ld, vb);
+  for (int k = 0; k <= i; ++k) {
+    stage_async(X + (size_t)ci * NB * ld + (size_t)(c0 + k) * NB, ld, sA, LDA);
+    store_tile_transposed(vb, sB);
+    if (k < i) load_tile_regs(X + (size_t)aj * NB * ld + (size_t)(c0 + k + 1) * NB, ld, vb);
+    cp_async_wait_all();
+    __syncthreads();
+    TileMMA<T>::sub(sA, sB, acc);  // acc = -X_CC U
+    __syncthreads();
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
+  store_acc(X + (size_t)ci * NB * ld + (size_t)aj * NB, ld, acc);
+}
+
+// Tiles of level s (host side of level_tile).
+inline int level_tiles(int nt, int s) {
+  int n = 0;
+  for (int c0 = s; c0 < nt; c0 += 2 * s) n += std::min(s, nt - c0) * s;
+  return n;
 }
 
 // out_IJ = scale (X^T X)_IJ = scale sum_{k >= I} X_kI^T X_kJ for the lower
@@ -1651,7 +1687,8 @@ __global__ void b_invdiag_kernel(const T* __restrict__ G, int ld, int nt, T inv_
 template <typename T>
 int set_tc_smem() {
   constexpr int smem = (int)tc_smem_bytes<T>();
-  PBG_CUDA_TRY(cudaFuncSetAttribute(trsm_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_level_u_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_level_x_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   PBG_CUDA_TRY(cudaFuncSetAttribute(lauum_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   return PBG_OK;
 }
@@ -1661,9 +1698,13 @@ int trtri_tc(const T* L, const T* invdiag, T* X, int ld, cudaStream_t st) {
   const int nt = ld / NB;
   constexpr size_t smem = tc_smem_bytes<T>();
   if (int rc = set_tc_smem<T>()) return rc;
-  PBG_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)ld * ld * sizeof(T), st));
-  for (int k = -1; k + 1 < nt; ++k) {
-    trsm_step_kernel<T><<<(nt - k - 1) * (k + 1) + 1, THREADS, smem, st>>>(L, invdiag, k, X, ld, nt);
+  trtri_diag_kernel<T><<<nt, THREADS, 0, st>>>(invdiag, X, ld);
+  PBG_CHECK_LAUNCH();
+  for (int s = 1; s < nt; s *= 2) {
+    const int tiles = level_tiles(nt, s);
+    trtri_level_u_kernel<T><<<tiles, THREADS, smem, st>>>(L, X, ld, nt, s);
+    PBG_CHECK_LAUNCH();
+    trtri_level_x_kernel<T><<<tiles, THREADS, smem, st>>>(X, ld, nt, s);
     PBG_CHECK_LAUNCH();
   }
   return PBG_OK;

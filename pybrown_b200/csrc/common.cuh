@@ -34,6 +34,9 @@
 void pbg_record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 void pbg_set_error_message(const char* fmt, ...);
 void pbg_count_launch();
+// Adds n launches (kernels replayed inside a CUDA graph; negative to take
+// back the launches a stream capture counted without running them).
+void pbg_count_launches(long long n);
 
 // Device-side error bits (written with atomicOr into a status word).
 enum : unsigned {

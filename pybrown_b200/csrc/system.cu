@@ -142,7 +142,7 @@ void destroy_system(pbg_system* s) {
                   s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
                   s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
                   s->chol_work, s->inv_work, s->dflags, s->div, s->sol, s->sol0, s->res, s->corr,
-                  s->G,    s->Ginv};
+                  s->G};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
@@ -200,10 +200,7 @@ int create_system(const pbg_params* prm, pbg_system** out) {
       SYS_ALLOC(s->R0, mat * sizeof(double));
     }
     SYS_ALLOC(s->inv_work, s->mlub ? tc_inverse_work_bytes(s->ld) : spd_inverse_work_bytes(s->ld));
-    if (s->mlub) {
-      SYS_ALLOC(s->G, mat * sizeof(float));
-      SYS_ALLOC(s->Ginv, (size_t)PBG_TILE * ld * sizeof(float));
-    }
+    if (s->mlub && p.propagation_scheme == PBG_SCHEME_MIDPOINT) SYS_ALLOC(s->G, mat * sizeof(float));
   }
   double** vecs[] = {&s->FX, &s->U,  &s->BX,   &s->ddet, &s->y,   &s->rwork, &s->Dy,
                      &s->drift, &s->xi, &s->sol, &s->sol0, &s->res, &s->corr};
@@ -375,11 +372,11 @@ int decompose(pbg_system* s, cudaStream_t st) {
     const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
     if ((rc = tc_reversed_factor(w.X, w.F, s->ld, std::sqrt(s->p.kBT), (float*)s->B, (float*)s->chol_work, st)))
       return rc;
-    // keep G and its diagonal inverses: the noise products use them directly
-    PBG_CUDA_TRY(cudaMemcpyAsync(s->G, w.F, (size_t)s->ld * s->ld * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    PBG_CUDA_TRY(cudaMemcpyAsync(s->Ginv, w.invdiag, (size_t)PBG_TILE * s->ld * sizeof(float),
-                                 cudaMemcpyDeviceToDevice, st));
-    s->g_valid = true;
+    // keep G for the midpoint's inv(B0^T) xi
+    if (s->p.propagation_scheme == PBG_SCHEME_MIDPOINT) {
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->G, w.F, (size_t)s->ld * s->ld * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      s->g_valid = true;
+    }
     return PBG_OK;
   }
   const long long total = (long long)s->ld * s->ld;
@@ -605,21 +602,16 @@ static void midpoint_restore(pbg_system* s) {
   }
 }
 
-// Mixed lubricated path, from the FP32 factor G of J R0 J (backward-stable
-// triangular solve and product instead of the explicit FP32 B):
-//   U = B0 xi = sqrt(kBT) J G^{-T} J xi,   y = inv(B0^T) xi = J G J xi / sqrt(kBT).
-static int noise_from_G(pbg_system* s, cudaStream_t st) {
+// Mixed lubricated path, midpoint scheme: y = inv(B0^T) xi = J G J xi / sqrt(kBT)
+// by one triangular product with the FP32 factor G of J R0 J (instead of the
+// blocked triangular solve with B0).
+static int midpoint_y_from_G(pbg_system* s, cudaStream_t st) {
   const int ld = s->ld, g = (ld + 255) / 256;
-  const double sk = std::sqrt(s->p.kBT);
   reverse_scale_kernel<<<g, 256, 0, st>>>(s->xi, ld, 1.0, s->res);
   PBG_CHECK_LAUNCH();
-  int rc = launch_trsv_upper(s->G, ld, PBG_PREC_MIXED, s->Ginv, s->res, s->rwork, s->corr, st);
+  int rc = launch_trmv_lower(s->G, ld, ld, PBG_PREC_MIXED, s->res, s->corr, st);
   if (rc) return rc;
-  reverse_scale_kernel<<<g, 256, 0, st>>>(s->corr, ld, sk, s->U);
-  PBG_CHECK_LAUNCH();
-  if (s->p.propagation_scheme != PBG_SCHEME_MIDPOINT) return PBG_OK;
-  if ((rc = launch_trmv_lower(s->G, ld, ld, PBG_PREC_MIXED, s->res, s->corr, st))) return rc;
-  reverse_scale_kernel<<<g, 256, 0, st>>>(s->corr, ld, 1.0 / sk, s->y);
+  reverse_scale_kernel<<<g, 256, 0, st>>>(s->corr, ld, 1.0 / std::sqrt(s->p.kBT), s->y);
   PBG_CHECK_LAUNCH();
   return PBG_OK;
 }
@@ -633,12 +625,7 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
   const int n = s->n;
   int rc;
   PBG_CUDA_TRY(cudaMemcpyAsync(s->xi, xi, n * sizeof(double), cudaMemcpyDefault, st));
-  const bool from_G = s->mlub && s->g_valid;
-  if (from_G) {
-    if ((rc = noise_from_G(s, st))) return rc;
-  } else if ((rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st))) {
-    return rc;
-  }
+  if ((rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st))) return rc;
   bool overlap = false;
   if (s->p.propagation_scheme == PBG_SCHEME_ERMAK) {
     // box.py:219-248
@@ -674,7 +661,11 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
     return rc;
   }
   // stochastic drift m/2 sqrt(2 dt) (D' inv(B0^T) - B0) @ xi = c2 (D' y - B0 xi), B0^T y = xi
-  if (!from_G && (rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) return rc;
+  if (s->mlub && s->g_valid) {
+    if ((rc = midpoint_y_from_G(s, st))) return rc;
+  } else if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) {
+    return rc;
+  }
   if (s->mlub) {
     // B0 xi = D0 y, so the drift is c2 kBT (R'^{-1} y - R0^{-1} y): both terms
     // by refined solves, so that the FP32 rounding of B0 does not enter the
@@ -849,7 +840,7 @@ int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t s
     PBG_CUDA_TRY(cudaFreeAsync(stage, st));
   }
   if (which == PBG_MAT_R) s->work_holds_R = false;
-  if (which == PBG_MAT_B) s->g_valid = false;  // the noise then comes from the explicit B
+  if (which == PBG_MAT_B) s->g_valid = false;  // inv(B0^T) xi then comes from the explicit B
   return rc;
 }
 

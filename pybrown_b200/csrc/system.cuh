@@ -18,9 +18,8 @@ struct pbg_system {
   // (and their midpoint copies) are FP32, R stays FP64, D and B are FP32.
   bool mlub = false;
   bool work_holds_R = false;  // inv_work holds G = chol(J R J) and inv(G) of the current R
-  void* G = nullptr;          // mlub: FP32 G of the step-start R (noise factor B = sqrt(kBT) J G^{-T} J)
-  void* Ginv = nullptr;       // mlub: inverted diagonal tiles of G
-  bool g_valid = false;       // G and Ginv belong to the B in use
+  void* G = nullptr;          // mlub, midpoint: FP32 G of the step-start R (B = sqrt(kBT) J G^{-T} J)
+  bool g_valid = false;       // G belongs to the B in use
   int prec = PBG_PREC_FP64;  // element type of D and B
   size_t es = 8;
   const pbg::EwaldTables* tables = nullptr;

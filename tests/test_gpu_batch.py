@@ -218,6 +218,34 @@ def test_autotuned_schedule_changes_no_result(precision):
         assert np.array_equal(ref, run(sched)[0]), sched
 
 
+def test_graph_replay_matches_direct_launches():
+    """From the second step with an unchanged membership the start of a step
+    replays one CUDA graph; the trajectories equal, bit for bit, those of a
+    batch whose schedule is switched every step (a rebuild, so its kernels are
+    launched one by one)."""
+    from pybrown_b200.batch import ReplicaBatch
+    configs = [_config(600 + k, N, 0.05, 10.0, 30.0) for k, N in enumerate((64, 150, 90))]
+
+    def run(toggle):
+        batch = ReplicaBatch(precision="mixed")
+        slots = [batch.add(p, r, l, seed=30 + k, noise="device") for k, (p, r, l) in enumerate(configs)]
+        out, states = [], []
+        for step in range(5):
+            if toggle:
+                batch.set_schedule("added" if step % 2 else "larger_first")
+            batch.propagate(1.0)
+            states.append(batch.graph_state())
+            out.append(np.concatenate([batch.positions(s).ravel() for s in slots]))
+        batch.close()
+        return np.array(out), states
+
+    graph, g_states = run(False)
+    direct, d_states = run(True)
+    assert g_states == [0, 1, 1, 1, 1]
+    assert d_states == [0, 0, 0, 0, 0]
+    assert np.array_equal(graph, direct)
+
+
 def test_device_noise_is_standard_normal():
     """The counter-based stream has mean 0, variance 1 and no correlation
     between neighbouring draws, seen through the moves of a very dilute rpy
