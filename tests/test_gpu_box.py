@@ -174,3 +174,24 @@ def test_box_mixed_lubrication(oracle_lib, scheme):
     assert rel_err(box.Rff, ref.Rff) <= 5e-5
     assert rel_err(box.D, ref.D) <= 1e-4
     assert rel_err(box.B, ref.B) <= 1e-4
+
+
+def test_box_vs_oracle_stokesian_n256(oracle_lib):
+    """FP64 SD at N=256 (order 768, 12 tiles: every level of the tensor-core
+    triangular inverse down to 8-tile blocks) against the oracle."""
+    from oracle.oracle import OracleBox
+    N, a = 256, 20.0
+    L = (N * 4 * math.pi * a ** 3 / 3 / 0.30) ** (1 / 3)
+    pos, radii = _config(11, N, L, a, a, 0.05 * a)
+    inp = _inp(box_length=L, hydrodynamics="rpy_smith_lub", propagation_scheme="midpoint", lubrication_cutoff=0.5)
+    box = _box(pos, radii, inp)
+    ref = OracleBox(pos, radii, inp, clib=oracle_lib)
+    for _ in range(2):
+        box.propagate(0.1)
+        ref.propagate(0.1)
+        assert box.draw_count == ref.draw_count
+    got = np.array([b.r for b in box.beads])
+    assert rel_err(got - pos, ref.pos - pos) <= 1e-10
+    assert rel_err(box.Rff, ref.Rff) <= 1e-10
+    assert rel_err(box.D, ref.D) <= 1e-10
+    assert rel_err(box.B, ref.B) <= 1e-10
