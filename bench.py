@@ -382,12 +382,18 @@ def run_ours(args, torch, dist, rank, world):
         "cpu_baseline": cpu,
         "clocks": results["mixed"]["clocks"],
     }
-    if world == 1 and not args.no_lub:
-        line["lubrication"] = run_lub_section(args, torch)
-    if world == 1 and not args.no_batch:
-        line["batch"] = run_batch_section(args, torch)
-    if world == 1 and not args.no_serve:
-        line["serve"] = run_serve_section(args, torch)
+    # A failure in a secondary section is reported in its own key (with the
+    # library's error) instead of costing the whole line.
+    from pybrown_b200._lib import PbgError
+    sections = (("lubrication", args.no_lub, run_lub_section), ("batch", args.no_batch, run_batch_section),
+                ("serve", args.no_serve, run_serve_section))
+    for key, skip, fn in sections:
+        if world != 1 or skip:
+            continue
+        try:
+            line[key] = fn(args, torch)
+        except PbgError as e:
+            line[key] = {"error": str(e)}
     return line
 
 
