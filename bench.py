@@ -284,12 +284,27 @@ def cpu_reference_steps(N, steps, warmup, threads=None):
 CHOL_MIXED_TRAFFIC_BYTES = 19651072 + 2610432
 
 
+def replica_seed(rank):
+    """Each rank advances an independent replica of the workload."""
+    return WORKLOAD["seed"] + rank
+
+
+def max_over_ranks(torch, dist, value, device="cuda"):
+    """The slowest rank's time (every rank takes part; identity without a
+    process group)."""
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, torch, dist, rank, world):
     from pybrown_b200 import _lib
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     N = WORKLOAD["n_beads"]
-    seed = WORKLOAD["seed"] + rank  # independent replica per rank
+    seed = replica_seed(rank)
     pos, radii = bead_config(seed, N, WORKLOAD["box_length"], 10.0, 40.0)
     dt = WORKLOAD["dt"]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -314,10 +329,7 @@ def run_ours(args, torch, dist, rank, world):
             sampler.__exit__(None, None, None)
         launches = _lib.lib.pbg_launch_count() - launches0
         barrier()
-        if dist is not None:
-            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(torch, dist, ms)
         results[prec] = {"ms": ms, "launches": launches, "run": run,
                          "clocks": sampler.summary() if sampler else None}
 
@@ -339,10 +351,7 @@ def run_ours(args, torch, dist, rank, world):
         box.propagate(dt)
     barrier()
     e2e_ms = timed_steps(torch, lambda: box.propagate(dt), args.steps, flush)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(torch, dist, e2e_ms)
 
     # dominant kernel: the Cholesky factorisation of D (3072 x 3072)
     chol_ms, info = cholesky_kernel_timing(torch, results["mixed"]["run"].box, 3)
