@@ -51,7 +51,8 @@ constexpr int TILE_PER_THREAD = 64 * 64 / THREADS;  // elements of a 64 x 64 til
 constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
-enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3 };
+// TASK_U2: U(i, j, k) and U(i+1, j, k) as one task (they share L_jk).
+enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3, TASK_U2 = 4 };
 
 struct DFArgs {
   void* A;
@@ -992,6 +993,36 @@ __device__ __forceinline__ void update_tile(const DFArgs& a, int i, int j, int k
   store_tile(sC, LDA, tile<T>(a, i, j), a.ld);
 }
 
+// U(i, j, k) and U(i+1, j, k) together: five tiles (L_ik, L_jk, L_{i+1,k} and
+// both targets) staged with 16-byte copies in one round, two accumulators
+// against the shared L_jk, one round of 16-byte stores.  s: five [64][LDA]
+// T tiles.
+template <typename T>
+__device__ __forceinline__ void update_tile_pair(const DFArgs& a, int i, int j, int k, T acc[16], T* s) {
+  T* sA1 = s;
+  T* sB = sA1 + NB * LDA;
+  T* sC1 = sB + NB * LDA;
+  T* sA2 = sC1 + NB * LDA;
+  T* sC2 = sA2 + NB * LDA;
+  if (i != j) stage_async(tile<T>(a, i, k), a.ld, sA1, LDA);
+  stage_async(tile<T>(a, j, k), a.ld, sB, LDA);
+  stage_async(tile<T>(a, i + 1, k), a.ld, sA2, LDA);
+  stage_async(tile<T>(a, i, j), a.ld, sC1, LDA);
+  stage_async(tile<T>(a, i + 1, j), a.ld, sC2, LDA);
+  cp_async_wait_all();
+  __syncthreads();
+  T acc2[16];
+  smem_to_acc(sC1, acc);
+  smem_to_acc(sC2, acc2);
+  TileMMA<T>::sub(i != j ? sA1 : sB, sB, acc);
+  TileMMA<T>::sub(sA2, sB, acc2);
+  acc_to_smem(acc, sC1);  // each thread rewrites the elements it read
+  acc_to_smem(acc2, sC2);
+  __syncthreads();
+  store_tile(sC1, LDA, tile<T>(a, i, j), a.ld);
+  store_tile(sC2, LDA, tile<T>(a, i + 1, j), a.ld);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1048,6 +1079,20 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
       TRACE(1, t);
       update_tile(a, i, j, k, acc, sA, sB, sB + NB * LDA);
       publish(a.upd + i * nt + j, k + 1);
+      TRACE(2, t);
+    } else if (type == TASK_U2) {
+      // U(i, j, k) and U(i+1, j, k): L_ik, L_{i+1,k}, L_jk final, k previous updates of both
+      const int* fl[5] = {a.fin + i * nt + k, a.fin + (i + 1) * nt + k, a.fin + j * nt + k, a.upd + i * nt + j,
+                          a.upd + (i + 1) * nt + j};
+      const int tg[5] = {1, 1, 1, k, k};
+      if (!wait_all(a, fl, tg, 5, &s_ok)) return;
+      TRACE(1, t);
+      update_tile_pair(a, i, j, k, acc, sA);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        st_release(a.upd + i * nt + j, k + 1);
+        st_release(a.upd + (i + 1) * nt + j, k + 1);
+      }
       TRACE(2, t);
     } else {
       // S(i, j), i >= j + 2: the tile after its last update, times inv(L_jj)^T
@@ -1188,8 +1233,12 @@ int get_task_table(int nt, const int4** out, int* count) {
     // the rest of column k+1 of the update with panel k is fused into F(k+1)
     // and the workers' S(., k+1); the plain updates cover columns >= k+2, the
     // one gating the next panel first
-    for (int jj = k + 2; jj < nt; ++jj)
-      for (int i = jj; i < nt; ++i) t.push_back(make_int4(TASK_U, i, jj, k));
+    // (rows paired: U(i, jj, k) and U(i+1, jj, k) share L_jj,k)
+    for (int jj = k + 2; jj < nt; ++jj) {
+      int i = jj;
+      for (; i + 1 < nt; i += 2) t.push_back(make_int4(TASK_U2, i, jj, k));
+      if (i < nt) t.push_back(make_int4(TASK_U, i, jj, k));
+    }
   }
   int4* d = nullptr;
   if (!t.empty()) {
@@ -1207,7 +1256,7 @@ int get_task_table(int nt, const int4** out, int* count) {
 
 template <typename T>
 size_t df_smem_bytes() {
-  return chain_smem_bytes<T>();
+  return std::max(chain_smem_bytes<T>(), 5 * NB * LDA * sizeof(T));  // the chain, or a paired update
 }
 
 // tasks_override / spin_limit: only for the wait-expiry self-test.
@@ -1293,7 +1342,7 @@ extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(l
   std::vector<int4> tasks(nfull);
   PBG_CUDA_TRY(cudaMemcpy(tasks.data(), full, nfull * sizeof(int4), cudaMemcpyDeviceToHost));
   const auto dropped = std::remove_if(tasks.begin(), tasks.end(), [](const int4& t) {
-    return t.x == TASK_U && t.y == 2 && t.z == 2 && t.w == 0;
+    return (t.x == TASK_U || t.x == TASK_U2) && t.y == 2 && t.z == 2 && t.w == 0;
   });
   if (dropped == tasks.end()) return PBG_ERR_STATE;
   tasks.erase(dropped, tasks.end());
