@@ -280,8 +280,8 @@ def cpu_reference_steps(N, steps, warmup, threads=None):
 # from one ncu capture of the same kernel on the same order:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:chol_df -c 1 --clock-control none \
 #       python -m pybrown_b200.profile_cases cholesky --order 3072 --precision mixed
-# (19,651,072 + 2,610,432 B); re-measure when the factorisation changes.
-CHOL_MIXED_TRAFFIC_BYTES = 19651072 + 2610432
+# (19,544,320 + 2,230,272 B); re-measure when the factorisation changes.
+CHOL_MIXED_TRAFFIC_BYTES = 19544320 + 2230272
 
 
 def replica_seed(rank):
