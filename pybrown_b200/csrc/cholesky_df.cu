@@ -343,8 +343,7 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 }
 template <>
 __device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt_nr(x); }
-template <>
-__device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
+
 
 // Panel strip row length: 8 values padded so that 16-byte row loads and the
 // tensor-core fragment loads of eight different rows hit distinct banks.
@@ -389,45 +388,10 @@ __device__ __forceinline__ void strip_update(const double* P, int lo, double acc
   }
 }
 
-__device__ __forceinline__ void strip_update(const float* P, int lo, float acc[16]) {
-  constexpr int PB = Strip<float>::PB;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1), g = lane >> 2, t = lane & 3;
-  unsigned ah[4], al[4];
-  {
-    const int r0 = m0 + g, r1 = m0 + g + 8;
-    const float v[4] = {r0 >= lo ? -P[r0 * PB + t] : 0.f, r1 >= lo ? -P[r1 * PB + t] : 0.f,
-                        r0 >= lo ? -P[r0 * PB + t + 4] : 0.f, r1 >= lo ? -P[r1 * PB + t + 4] : 0.f};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      ah[q] = to_tf32(v[q]);
-      al[q] = to_tf32(v[q] - __uint_as_float(ah[q]));
-    }
-  }
-#pragma unroll
-  for (int nt = 0; nt < 4; ++nt) {
-    const int c = n0 + 8 * nt + g;
-    const float v0 = c >= lo ? P[c * PB + t] : 0.f;
-    const float v1 = c >= lo ? P[c * PB + t + 4] : 0.f;
-    const unsigned bh0 = to_tf32(v0), bh1 = to_tf32(v1);
-    const unsigned bl0 = to_tf32(v0 - __uint_as_float(bh0)), bl1 = to_tf32(v1 - __uint_as_float(bh1));
-    float* cc = acc + 4 * nt;
-#define PBG_TF32_MMA(A0, A1, A2, A3, B0, B1)                                                        \
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, " \
-               "{%8,%9}, {%0,%1,%2,%3};"                                                            \
-               : "+f"(cc[0]), "+f"(cc[1]), "+f"(cc[2]), "+f"(cc[3])                                 \
-               : "r"(A0), "r"(A1), "r"(A2), "r"(A3), "r"(B0), "r"(B1))
-    PBG_TF32_MMA(al[0], al[1], al[2], al[3], bh0, bh1);
-    PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bl0, bl1);
-    PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bh0, bh1);
-#undef PBG_TF32_MMA
-  }
-}
-
 // One warp's output tile D = A B of a small smem product on the tensor cores:
 // A rows with stride lda (k contiguous), B k-major rows with stride ldb, K a
-// multiple of 8.  FP64: an 8 x 8 tile (mma m8n8k4), lane holds D[g][2t + h];
-// FP32: a 16 x 8 tile (3xTF32 mma m16n8k8), lane holds D[g + 8i][2t + h].
+// multiple of 4: an 8 x 8 FP64 tile (mma m8n8k4), lane holds D[g][2t + h].
+// (The diagonal tiles are inverted in FP64 in both paths.)
 struct WarpTile64 {
   static constexpr int TM = 8;
   static __device__ __forceinline__ void mma(const double* A, int lda, const double* B, int ldb, int K, double d[4]) {
@@ -446,45 +410,8 @@ struct WarpTile64 {
   static constexpr int NQ = 2;
 };
 
-struct WarpTile32 {
-  static constexpr int TM = 16;
-  static __device__ __forceinline__ void mma(const float* A, int lda, const float* B, int ldb, int K, float d[4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    d[0] = d[1] = d[2] = d[3] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += 8) {
-      const float va[4] = {A[g * lda + k0 + t], A[(g + 8) * lda + k0 + t], A[g * lda + k0 + t + 4],
-                           A[(g + 8) * lda + k0 + t + 4]};
-      const float vb[2] = {B[(k0 + t) * ldb + g], B[(k0 + t + 4) * ldb + g]};
-      unsigned ah[4], al[4], bh[2], bl[2];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        ah[q] = to_tf32(va[q]);
-        al[q] = to_tf32(va[q] - __uint_as_float(ah[q]));
-      }
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        bh[q] = to_tf32(vb[q]);
-        bl[q] = to_tf32(vb[q] - __uint_as_float(bh[q]));
-      }
-#define PBG_TF32_MMA(A0, A1, A2, A3, B0, B1)                                                        \
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, " \
-               "{%8,%9}, {%0,%1,%2,%3};"                                                            \
-               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])                                     \
-               : "r"(A0), "r"(A1), "r"(A2), "r"(A3), "r"(B0), "r"(B1))
-      PBG_TF32_MMA(al[0], al[1], al[2], al[3], bh[0], bh[1]);
-      PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bl[0], bl[1]);
-      PBG_TF32_MMA(ah[0], ah[1], ah[2], ah[3], bh[0], bh[1]);
-#undef PBG_TF32_MMA
-    }
-  }
-  static __device__ __forceinline__ int row(int q) { return ((threadIdx.x & 31) >> 2) + 8 * (q >> 1); }
-  static __device__ __forceinline__ int col(int q) { return 2 * (threadIdx.x & 3) + (q & 1); }
-  static constexpr int NQ = 4;
-};
-
 template <typename T> struct WarpTileOf;
 template <> struct WarpTileOf<double> { using type = WarpTile64; };
-template <> struct WarpTileOf<float> { using type = WarpTile32; };
 
 // Inverse of the lower-triangular L_kk (in Lk, [64][LDA], zero above the
 // diagonal) into X ([64][LDA]), with Rinv[j] = 1 / L_jj and scratch Tm
