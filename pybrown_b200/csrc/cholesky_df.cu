@@ -101,29 +101,48 @@ __device__ __forceinline__ int smid() {
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 
-// Thread 0 waits until every flags[q] >= targets[q] (bounded); returns false
-// if the run was aborted.  The acquire loads by thread 0 followed by the CTA
-// barrier order every thread's later reads after the producers' release.
+// Warp 0 waits until every flags[q] >= targets[q] (count <= 5, bounded);
+// returns false if the run was aborted.  Lane q polls flag q, so one round
+// costs one L2 round trip whatever the count.  The acquire loads followed by
+// the CTA barrier order every thread's later reads after the producers'
+// release.
 __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* targets, int count, int* s_ok) {
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const int* flag = nullptr;
+    int target = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q)  // compile-time indices: the arrays stay in registers
+      if (q < count && q == lane) {
+        flag = flags[q];
+        target = targets[q];
+      }
+    bool done = flag == nullptr;
     int ok = 1;
-    for (int q = 0; q < count && ok; ++q) {
-      long long it = 0;
-      while (ld_acquire(flags[q]) < targets[q]) {
-        // the abort flag is polled every 16th round, so a round costs one L2 trip
-        if ((it & 15) == 15 && ld_acquire(a.ctl + 1)) { ok = 0; break; }
-        if (++it > a.spin_limit) {
+    for (long long it = 0;; ++it) {
+      if (!done) done = ld_acquire(flag) >= target;
+      if (__all_sync(0xffffffffu, done)) break;
+      // the abort flag is polled every 16th round, so a round costs one L2 trip
+      if ((it & 15) == 15) {
+        const int ab = __shfl_sync(0xffffffffu, lane == 0 ? ld_acquire(a.ctl + 1) : 0, 0);
+        if (ab) {
+          ok = 0;
+          break;
+        }
+      }
+      if (it + 1 > a.spin_limit) {
+        if (lane == 0) {
           atomicExch(a.ctl + 1, 1);
           atomicAdd(a.ctl + 2, 1);
           atomicOr(a.err, PBG_DEV_ERR_BARRIER);
           atomicCAS(a.info, 0, -1);  // -1: the factorisation gave up waiting
-          ok = 0;
-          break;
         }
-        if (it > 256) __nanosleep(200);
+        ok = 0;
+        break;
       }
+      if (it > 256) __nanosleep(200);
     }
-    *s_ok = ok;
+    if (lane == 0) *s_ok = ok;
   }
   __syncthreads();
   return *s_ok != 0;
