@@ -339,7 +339,7 @@ __global__ void gather_tasks_kernel(const GatherSeg* __restrict__ segs, int nseg
     const GatherSeg g = segs[s];
     for (int t = threadIdx.x; t < g.count; t += blockDim.x) {
       int4 v = g.src[t];
-      v.x = (v.x & 3) | (g.replica << 2);
+      v.x = (v.x & 7) | (g.replica << 3);
       out[g.dst + t] = v;
     }
   }

@@ -1072,7 +1072,8 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
 // inverse) over the same bytes and the FP64 factor scratch after them.
 template <typename T>
 constexpr size_t batch_smem_bytes() {
-  return sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>());
+  return std::max(sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>()),
+                  5 * NB * LDA * sizeof(T));  // or a paired update's five tiles
 }
 
 // Two CTAs per SM in the mixed path: a second task in flight per SM hides
@@ -1097,8 +1098,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
     __syncthreads();
     if (t >= ntasks) return;
     const int4 tk = tasks[t];
-    const int type = tk.x & 3, i = tk.y, j = tk.z, k = tk.w;
-    const CholRep& R = reps[tk.x >> 2];
+    const int type = tk.x & 7, i = tk.y, j = tk.z, k = tk.w;
+    const CholRep& R = reps[tk.x >> 3];
     DFArgs a;
     a.A = R.A;
     a.ld = R.ld;
@@ -1126,6 +1127,17 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
         store_acc(tile<T>(a, i, j), a.ld, acc);
       }
       publish(a.upd + i * nt + j, k + 1);
+    } else if (type == TASK_U2) {
+      const int* fl[5] = {a.fin + i * nt + k, a.fin + (i + 1) * nt + k, a.fin + j * nt + k, a.upd + i * nt + j,
+                          a.upd + (i + 1) * nt + j};
+      const int tg[5] = {1, 1, 1, k, k};
+      if (!wait_all(a, fl, tg, 5, &s_ok)) return;
+      update_tile_pair(a, i, j, k, acc, sA);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        st_release(a.upd + i * nt + j, k + 1);
+        st_release(a.upd + (i + 1) * nt + j, k + 1);
+      }
     } else {
       const int col = j;
       if (col > 0) {
@@ -1401,8 +1413,11 @@ void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& 
     seg_start.push_back((int)tasks.size());
     tasks.push_back(make_int4(TASK_F, k + 1, k + 1, k + 1));
     seg_start.push_back((int)tasks.size());
-    for (int jj = k + 2; jj < nt; ++jj)
-      for (int i = jj; i < nt; ++i) tasks.push_back(make_int4(TASK_U, i, jj, k));
+    for (int jj = k + 2; jj < nt; ++jj) {  // rows paired, as in the single-matrix list
+      int i = jj;
+      for (; i + 1 < nt; i += 2) tasks.push_back(make_int4(TASK_U2, i, jj, k));
+      if (i < nt) tasks.push_back(make_int4(TASK_U, i, jj, k));
+    }
     seg_start.push_back((int)tasks.size());
     for (int i = k + 2; i < nt; ++i) tasks.push_back(make_int4(TASK_S, i, k + 1, k + 1));
   }

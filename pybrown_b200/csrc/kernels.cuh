@@ -154,7 +154,7 @@ struct CholRep {
 };
 // One replica's task list (task.x = type, replica tag 0) cut into segments
 // that a batch interleaves with the other replicas' (see cholesky_df.cu);
-// task.x = type | replica << 2 in the merged list.
+// task.x = type | replica << 3 in the merged list.
 void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start);
 // ctl: 4 ints (next task, abort, spin failures, error bits), zero before the launch.
 // ctas_per_sm: resident CTAs per SM (0 = as many as fit).
