@@ -406,6 +406,35 @@ def run_ours(args, torch, dist, rank, world):
     return line
 
 
+def cpu_reference_lub_steps(steps=1):
+    """The reference's CPU path on the lubricated workload: its C library
+    (OpenMP build in oracle/_ref) for the tensors, NumPy LAPACK for the
+    inverses and the Cholesky, driven like Box.propagate (midpoint).  Returns
+    (steps/s, cores, kind, sample)."""
+    from oracle.oracle import REF_OMP_LIB, REF_LIB, ORACLE_LIB, CLib, OracleBox
+    cores = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    lib, kind = None, "reference"
+    for path in (REF_OMP_LIB, REF_LIB):
+        if os.path.exists(path):
+            lib = CLib(path)
+            break
+    if lib is None:
+        lib, kind = CLib(ORACLE_LIB), "port"
+    w = lub_workload()
+    pos, radii = bead_config(w["seed"], w["n_beads"], w["box_length"], w["radius"], w["radius"], gap=w["min_gap"])
+    inp = lub_input("fp64")
+    inp.pop("precision", None)
+    box = OracleBox(pos, radii, inp, clib=lib)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        box.propagate(w["dt"])
+    dt = time.perf_counter() - t0
+    sample = (f"{steps} midpoint Box.propagate step(s) of the lubricated N=512 workload; "
+              f"{os.path.basename(lib.path)} + NumPy inv/cholesky, OMP threads={cores}")
+    return steps / dt, cores, kind, sample
+
+
 def run_lub_section(args, torch, precisions=("fp64", "mixed")):
     """The lubricated workload (lub_workload) stepped on the device: per-step
     CUDA events with an L2 flush between steps, like the main workload."""
@@ -429,6 +458,9 @@ def run_lub_section(args, torch, precisions=("fp64", "mixed")):
         d_mix -= w["box_length"] * np.round((d_mix - d_ref) / w["box_length"])
         out["mixed_vs_fp64_displacement_rel_err"] = float(np.max(np.abs(d_mix - d_ref)) / np.max(np.abs(d_ref)))
         out["mixed_over_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    if not args.no_cpu_baseline:
+        sps, cores, kind, sample = cpu_reference_lub_steps(steps=1)
+        out["cpu_baseline"] = {"value": sps, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample}
     return out
 
 
