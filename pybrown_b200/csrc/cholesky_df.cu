@@ -51,8 +51,9 @@ constexpr int TILE_PER_THREAD = 64 * 64 / THREADS;  // elements of a 64 x 64 til
 constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
-// TASK_U2: U(i, j, k) and U(i+1, j, k) as one task (they share L_jk).
-enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3, TASK_U2 = 4 };
+// TASK_U2 / TASK_U3: U(i, j, k), U(i+1, j, k) (and U(i+2, j, k)) as one task
+// (they share L_jk).  Triples only in the FP32 single-matrix list.
+enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3, TASK_U2 = 4, TASK_U3 = 5 };
 
 struct DFArgs {
   void* A;
@@ -101,7 +102,7 @@ __device__ __forceinline__ int smid() {
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 
-// Warp 0 waits until every flags[q] >= targets[q] (count <= 5, bounded);
+// Warp 0 waits until every flags[q] >= targets[q] (count <= 7, bounded);
 // returns false if the run was aborted.  Lane q polls flag q, so one round
 // costs one L2 round trip whatever the count.  The acquire loads followed by
 // the CTA barrier order every thread's later reads after the producers'
@@ -112,7 +113,7 @@ __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* ta
     const int* flag = nullptr;
     int target = 0;
 #pragma unroll
-    for (int q = 0; q < 5; ++q)  // compile-time indices: the arrays stay in registers
+    for (int q = 0; q < 7; ++q)  // compile-time indices: the arrays stay in registers
       if (q < count && q == lane) {
         flag = flags[q];
         target = targets[q];
@@ -969,6 +970,37 @@ __device__ __forceinline__ void update_tile_pair(const DFArgs& a, int i, int j, 
   store_tile(sC2, LDA, tile<T>(a, i + 1, j), a.ld);
 }
 
+// U(i, j, k), U(i+1, j, k), U(i+2, j, k) together: seven tiles in one round of
+// 16-byte copies, three accumulators against the shared L_jk.  s: seven
+// [64][LDA] T tiles.
+template <typename T>
+__device__ __forceinline__ void update_tile_triple(const DFArgs& a, int i, int j, int k, T acc[16], T* s) {
+  T* sB = s;
+  T* sA[3] = {s + NB * LDA, s + 2 * NB * LDA, s + 3 * NB * LDA};
+  T* sC[3] = {s + 4 * NB * LDA, s + 5 * NB * LDA, s + 6 * NB * LDA};
+  stage_async(tile<T>(a, j, k), a.ld, sB, LDA);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    if (r > 0 || i != j) stage_async(tile<T>(a, i + r, k), a.ld, sA[r], LDA);
+    stage_async(tile<T>(a, i + r, j), a.ld, sC[r], LDA);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  T acc2[16], acc3[16];
+  smem_to_acc(sC[0], acc);
+  smem_to_acc(sC[1], acc2);
+  smem_to_acc(sC[2], acc3);
+  TileMMA<T>::sub(i != j ? sA[0] : sB, sB, acc);
+  TileMMA<T>::sub(sA[1], sB, acc2);
+  TileMMA<T>::sub(sA[2], sB, acc3);
+  acc_to_smem(acc, sC[0]);  // each thread rewrites the elements it read
+  acc_to_smem(acc2, sC[1]);
+  acc_to_smem(acc3, sC[2]);
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 3; ++r) store_tile(sC[r], LDA, tile<T>(a, i + r, j), a.ld);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1038,6 +1070,21 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
       if (threadIdx.x == 0) {
         st_release(a.upd + i * nt + j, k + 1);
         st_release(a.upd + (i + 1) * nt + j, k + 1);
+      }
+      TRACE(2, t);
+    } else if (sizeof(T) == 4 && type == TASK_U3) {  // FP32 lists only: seven tiles of shared memory
+      const int* fl[7] = {a.fin + i * nt + k,       a.fin + (i + 1) * nt + k,       a.fin + (i + 2) * nt + k,
+                          a.fin + j * nt + k,       a.upd + i * nt + j,             a.upd + (i + 1) * nt + j,
+                          a.upd + (i + 2) * nt + j};
+      const int tg[7] = {1, 1, 1, 1, k, k, k};
+      if (!wait_all(a, fl, tg, 7, &s_ok)) return;
+      TRACE(1, t);
+      update_tile_triple(a, i, j, k, acc, sA);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        st_release(a.upd + i * nt + j, k + 1);
+        st_release(a.upd + (i + 1) * nt + j, k + 1);
+        st_release(a.upd + (i + 2) * nt + j, k + 1);
       }
       TRACE(2, t);
     } else {
@@ -1170,9 +1217,11 @@ std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
 // Task list of the worker CTAs for an nt x nt tile grid (see the file comment).
-int get_task_table(int nt, const int4** out, int* count) {
+// group: updates per task down a column (2, or 3 for the FP32 kernel).
+int get_task_table(int nt, int group, const int4** out, int* count) {
   std::lock_guard<std::mutex> lk(g_task_mu);
-  auto it = g_task_tables.find(nt);
+  const int key = nt * 4 + group;
+  auto it = g_task_tables.find(key);
   if (it != g_task_tables.end()) {
     *out = it->second.first;
     *count = it->second.second;
@@ -1191,9 +1240,11 @@ int get_task_table(int nt, const int4** out, int* count) {
     // the rest of column k+1 of the update with panel k is fused into F(k+1)
     // and the workers' S(., k+1); the plain updates cover columns >= k+2, the
     // one gating the next panel first
-    // (rows paired: U(i, jj, k) and U(i+1, jj, k) share L_jj,k)
+    // (rows grouped: U(i, jj, k), U(i+1, jj, k) [, U(i+2, jj, k)] share L_jj,k)
     for (int jj = k + 2; jj < nt; ++jj) {
       int i = jj;
+      if (group == 3)
+        for (; i + 2 < nt; i += 3) t.push_back(make_int4(TASK_U3, i, jj, k));
       for (; i + 1 < nt; i += 2) t.push_back(make_int4(TASK_U2, i, jj, k));
       if (i < nt) t.push_back(make_int4(TASK_U, i, jj, k));
     }
@@ -1206,7 +1257,7 @@ int get_task_table(int nt, const int4** out, int* count) {
     }
     PBG_CUDA_TRY(cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
-  g_task_tables[nt] = std::make_pair(d, (int)t.size());
+  g_task_tables[key] = std::make_pair(d, (int)t.size());
   *out = d;
   *count = (int)t.size();
   return PBG_OK;
@@ -1214,7 +1265,8 @@ int get_task_table(int nt, const int4** out, int* count) {
 
 template <typename T>
 size_t df_smem_bytes() {
-  return std::max(chain_smem_bytes<T>(), 5 * NB * LDA * sizeof(T));  // the chain, or a paired update
+  // the chain, or a grouped update (three in FP32, two in FP64)
+  return std::max(chain_smem_bytes<T>(), (sizeof(T) == 4 ? 7 : 5) * NB * LDA * sizeof(T));
 }
 
 // tasks_override / spin_limit: only for the wait-expiry self-test.
@@ -1228,7 +1280,7 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
     tasks = tasks_override;
     ntasks = ntasks_override;
   } else {
-    int rc = get_task_table(nt, &tasks, &ntasks);
+    int rc = get_task_table(nt, sizeof(T) == 4 ? 3 : 2, &tasks, &ntasks);
     if (rc) return rc;
   }
   const size_t smem = df_smem_bytes<T>();
@@ -1295,7 +1347,7 @@ extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(l
   if (spin_limit < 1 || spin_limit > (1LL << 24)) return PBG_ERR_ARG;
   const int4* full = nullptr;
   int nfull = 0;
-  int rc = get_task_table(nt, &full, &nfull);
+  int rc = get_task_table(nt, 2, &full, &nfull);
   if (rc) return rc;
   std::vector<int4> tasks(nfull);
   PBG_CUDA_TRY(cudaMemcpy(tasks.data(), full, nfull * sizeof(int4), cudaMemcpyDeviceToHost));
