@@ -793,7 +793,11 @@ static int enqueue_begin(pbg_batch* b, double dt, int build_D, int cholesky, boo
 static int capture_begin(pbg_batch* b, double dt, int build_D, int cholesky, bool any_force) {
   if (!b->cap_stream) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   const long long l0 = pbg_launch_count();
-  PBG_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeRelaxed));
+  if (cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    b->graph_refused = true;
+    return PBG_OK;
+  }
   int rc = enqueue_begin(b, dt, build_D, cholesky, any_force, b->cap_stream);
   cudaGraph_t graph = nullptr;
   const cudaError_t end = cudaStreamEndCapture(b->cap_stream, &graph);
