@@ -1796,9 +1796,13 @@ int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* ou
   return lauum_tc<float>((const float*)X, ld, (float)scale, reversed, (float*)out, st);
 }
 
+// The data-flow scratch rounded up to 256 bytes, so X and F start aligned
+// whatever the tile count (the scratch itself is 80 + 8 nt^2 bytes).
+static size_t tc_scratch_bytes(int ld) { return (df_work_bytes(ld) + 255) / 256 * 256; }
+
 size_t tc_inverse_work_bytes(int ld) {
   const size_t nt = ld / NB;
-  return nt * NB * NB * sizeof(float) + df_work_bytes(ld) + 2 * (size_t)ld * ld * sizeof(float);
+  return nt * NB * NB * sizeof(float) + tc_scratch_bytes(ld) + 2 * (size_t)ld * ld * sizeof(float);
 }
 
 TcInverseWork tc_inverse_work(void* work, int ld) {
@@ -1807,7 +1811,7 @@ TcInverseWork tc_inverse_work(void* work, int ld) {
   TcInverseWork w;
   w.invdiag = reinterpret_cast<float*>(p);
   w.scratch = p + nt * NB * NB * sizeof(float);
-  w.X = reinterpret_cast<float*>(static_cast<unsigned char*>(w.scratch) + df_work_bytes(ld));
+  w.X = reinterpret_cast<float*>(static_cast<unsigned char*>(w.scratch) + tc_scratch_bytes(ld));
   w.F = w.X + (size_t)ld * ld;
   return w;
 }

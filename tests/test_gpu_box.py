@@ -176,6 +176,27 @@ def test_box_mixed_lubrication(oracle_lib, scheme):
     assert rel_err(box.B, ref.B) <= 1e-4
 
 
+def test_box_mixed_lubrication_odd_tile_count(oracle_lib):
+    """Mixed SD at N=48: order 144 padded to 192, an odd number (3) of 64-wide
+    tiles, so the tensor-core inverse's workspace offsets are not multiples of
+    an even tile count."""
+    from oracle.oracle import OracleBox
+    N, a = 48, 20.0
+    L = (N * 4 * math.pi * a ** 3 / 3 / 0.30) ** (1 / 3)
+    pos, radii = _config(5, N, L, a, a, 0.05 * a)
+    inp = _inp(box_length=L, hydrodynamics="rpy_smith_lub", propagation_scheme="midpoint", lubrication_cutoff=0.5)
+    box = _box(pos, radii, dict(inp, precision="mixed"))
+    ref = OracleBox(pos, radii, inp, clib=oracle_lib)
+    for _ in range(3):
+        box.propagate(0.1)
+        ref.propagate(0.1)
+        assert box.draw_count == ref.draw_count
+    got = np.array([b.r for b in box.beads])
+    assert rel_err(got - pos, ref.pos - pos) <= MLUB_BARS["midpoint"]
+    assert rel_err(box.D, ref.D) <= 1e-4
+    assert rel_err(box.B, ref.B) <= 1e-4
+
+
 def test_box_vs_oracle_stokesian_n256(oracle_lib):
     """FP64 SD at N=256 (order 768, 12 tiles: every level of the tensor-core
     triangular inverse down to 8-tile blocks) against the oracle."""
