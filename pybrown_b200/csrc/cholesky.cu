@@ -5,9 +5,9 @@
 // Storage: row-major, leading dimension ld (a multiple of 64), order padded to
 // ld with an identity block so every 64 x 64 tile is full.  The factorisation
 // itself is the data-flow kernel of cholesky_df.cu; this file adds the SPD
-// inverse inv(A) = inv(L)^T inv(L): triangular inversion by a right-looking
-// blocked solve, then the symmetric product, both on the tensor cores (FP64
-// DMMA tile products, cholesky_df.cu).
+// inverse inv(A) = inv(L)^T inv(L): triangular inversion level by level
+// (recursive doubling on the block structure), then the symmetric product,
+// both on the tensor cores (FP64 DMMA tile products, cholesky_df.cu).
 #include "common.cuh"
 #include "kernels.cuh"
 
