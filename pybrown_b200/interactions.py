@@ -331,6 +331,29 @@ def set_custom_interactions(input_data):
     return out
 
 
+def set_interactions(input_data, beads):
+    """interactions.py:483-513: the host Interactions of a simulation, in the
+    reference's order -- Lennard-Jones (6, 12 or 6-12, when switched on),
+    harmonic bonds and harmonic angles (when any bead has one), then the
+    custom ones.  The device path (DeviceInteractions) evaluates the built-in
+    terms itself; this list serves user code and host-side checks."""
+    out = []
+    lj6, lj12 = bool(input_data["lennard_jones_6"]), bool(input_data["lennard_jones_12"])
+    if lj6 or lj12:
+        pair = {(True, True): (LJ_6_12_force, LJ_6_12_energy),
+                (True, False): (LJ_6_attractive_force, LJ_6_attractive_energy),
+                (False, True): (LJ_12_repulsive_force, LJ_12_repulsive_energy)}[(lj6, lj12)]
+        out.append(Interactions(*pair, {"lennard_jones_alpha": input_data["lennard_jones_alpha"]}, bonded=False,
+                                how_many_body=2))
+    if any(len(b.bonded_with) > 0 for b in beads):
+        out.append(Interactions(harmonic_bond_force, harmonic_bond_energy, {}, bonded=True, how_many_body=2))
+    if any(len(b.angled_with) > 0 for b in beads):
+        out.append(Interactions(harmonic_angle_force, harmonic_angle_energy, {"box_length": input_data["box_length"]},
+                                bonded=True, how_many_body=3))
+    out.extend(set_custom_interactions(input_data))
+    return out
+
+
 class DeviceInteractions:
     """The pbg_interactions descriptor of the built-in interactions of a box
     (interactions.py:483-589) and the arrays it points to."""

@@ -5,8 +5,10 @@ interactions module (src/bdsim/pyBrown/interactions.py:641-849).
 
 Seeded bead pairs and triples (with bond and angle parameters and
 Lennard-Jones radii and well depths) go through the reference's harmonic
-bond / angle and LJ 6 / 12 / 6-12 force and energy functions; the results
-are stored as JSON for tests/test_interactions_golden.py.
+bond / angle and LJ 6 / 12 / 6-12 force and energy functions, and the whole
+host evaluation (set_interactions, then compute_forces_and_energy on the
+reference's pair vectors) runs over the same beads; the results are stored
+as JSON for tests/test_interactions_golden.py.
 """
 import json
 import math
@@ -75,6 +77,16 @@ def main():
     out["units"] = {"kcal_per_mole_to_joule": ref.kcal_per_mole_to_joule(2.5),
                     "joule_to_kcal_per_mole": ref.joule_to_kcal_per_mole(3.0e-21),
                     "eV_to_joule": ref.eV_to_joule(0.75), "joule_to_eV": ref.joule_to_eV(1.0e-19)}
+    # the whole host evaluation: set_interactions + compute_forces_and_energy
+    # over a bonded chain with angles and LJ 6-12 (all beads mobile)
+    inp = {"lennard_jones_6": True, "lennard_jones_12": True, "lennard_jones_alpha": alpha,
+           "custom_interactions": False, "box_length": L}
+    rij = np.asarray(bead_mod.compute_pointer_pbc_matrix(beads, L))
+    F = np.zeros(3 * len(beads))
+    E = 0.0
+    for inter in ref.set_interactions(inp, beads):
+        E += inter.compute_forces_and_energy(beads, rij, F)
+    out["full"] = {"input": inp, "pointers": rij.tolist(), "F": F.tolist(), "E": E}
     assert math.isfinite(out["angle_terms"][0]["energy"])
     with open(os.path.join(HERE, "interactions.json"), "w") as f:
         json.dump(out, f, indent=1)

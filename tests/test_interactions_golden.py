@@ -66,3 +66,19 @@ def test_unit_conversions(golden):
     assert I.joule_to_kcal_per_mole(3.0e-21) == u["joule_to_kcal_per_mole"]
     assert I.eV_to_joule(0.75) == u["eV_to_joule"]
     assert I.joule_to_eV(1.0e-19) == u["joule_to_eV"]
+
+
+def test_set_interactions_full_evaluation(golden):
+    """set_interactions + compute_forces_and_energy over a bonded chain with
+    angles and LJ 6-12, on the reference's pair vectors: same F and E."""
+    beads = _beads(golden)
+    full = golden["full"]
+    rij = np.array(full["pointers"])
+    F = np.zeros(3 * len(beads))
+    E = 0.0
+    inters = I.set_interactions(full["input"], beads)
+    assert [(i.how_many_body, i.bonded) for i in inters] == [(2, False), (2, True), (3, True)]
+    for inter in inters:
+        E += inter.compute_forces_and_energy(beads, rij, F)
+    assert F.tolist() == full["F"]
+    assert E == full["E"]
