@@ -39,6 +39,13 @@ WORKLOAD = {"workload": "BD-HI N=1024 polydisperse a~U[10,40] L=1500 Smith-Ewald
             "seed": 0}
 
 
+def bench_config(world):
+    """The `config` of the JSON line, identical in both arms (the reference
+    arm times the same workload on the host cores)."""
+    return dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
+                l2="GPU arm: L2 flushed between timed steps (256 MiB write)")
+
+
 def bead_config(seed, N, L, a_lo, a_hi, gap=0.0):
     """Sequential rejection sampling: radius, then a uniform position in
     [-L/2, L/2)^3, rejected if the minimum-image distance to any placed bead
@@ -374,8 +381,7 @@ def run_ours(args, torch, dist, rank, world):
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64 (mixed: FP32 tensor/trailing updates, FP64 diagonal tiles "
                                        "and positions)", "data": "synthetic (seeded bead configurations)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
-                       l2="flushed between timed steps (256 MiB write)"),
+        "config": bench_config(world),
         "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
         "mixed_vs_fp64_displacement_rel_err": rel_err,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
@@ -535,7 +541,7 @@ def run_reference(args, rank):
     return {"impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / sps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bead configurations)",
-            "config": dict(WORKLOAD, parallelism="host cores"),
+            "config": bench_config(args.gpus),
             "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

@@ -114,11 +114,13 @@ PBG_API int pbg_dev_smith_matrix(const double *pos, const double *radii, int n_b
  * by every GPU that loads it, until exit); nothing is allocated.  Limits:
  * at most 4096 real-space images, 2048 reciprocal half-vectors and
  * n_beads * (reciprocal half-vectors) * 16 bytes <= 4 MiB of phase tables
- * (e.g. 4096 beads at ewald_imag = 4); larger inputs return PBG_ERR_ARG.
- * The first call on a device looks up the array's device address (make it
- * before any stream capture).  Every call reuses the same array, so calls
- * that overlap on the GPU (different streams, or several host threads) race;
- * the array is fully rewritten by each call before it is read. */
+ * (e.g. 4096 beads at ewald_imag = 4); larger inputs (checked before any
+ * table is built) return PBG_ERR_ARG.  The lattice tables reach the array as
+ * kernel launch parameters, so no host buffer is staged and the host does not
+ * wait for the stream.  The first call on a device looks up the array's device
+ * address (make it before any stream capture).  Every call reuses the same
+ * array, so calls that overlap on the GPU (different streams, or several host
+ * threads) race; each call rewrites the parts it reads before reading them. */
 PBG_API int pbg_dev_smith_matrix_noalloc(const double *pos, const double *radii, int n_beads,
                                          double box_length, double alpha, int m_max, int n_max,
                                          double scale, int precision, void *M, int ld, void *stream);

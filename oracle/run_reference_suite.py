@@ -22,7 +22,8 @@ import sys
 import tempfile
 import unittest
 
-REFERENCE_BDSIM = "/root/reference/src/bdsim"
+# root of the reference checkout; PYBROWN_REFERENCE overrides the default
+REFERENCE_BDSIM = os.path.join(os.environ.get("PYBROWN_REFERENCE", "/root/reference"), "src", "bdsim")
 
 HOT_PATH_SUITES = [
     "test_diffusion_vs_python",

@@ -103,37 +103,6 @@ def pointer_pbc(bead1, bead2, box_size):
     return r
 
 
-def pole_pointer(bead1, bead2, bead3):
-    """bead.py:222-228: from the pole of bead2 (the point of its surface on the
-    far side from bead1, on the line through both centres) to bead3."""
-    shift = bead2.r - bead1.r
-    shift *= bead2.a / np.linalg.norm(shift)
-    return bead3.r - bead2.r - shift
-
-
-def pole_pointer_pbc(bead1, bead2, bead3, box_size):
-    """bead.py:258-268: pole_pointer with every component brought to the
-    minimum image by the same loops as pointer_pbc."""
-    r = pole_pointer(bead1, bead2, bead3)
-    for i in range(3):
-        r[i] = _min_image(r[i], box_size)
-    return r
-
-
-def angle_pbc(r12, r23):
-    """bead.py:272-278: the angle at the middle bead, in degrees, between the
-    bond vectors r12 (bead 1 -> 2) and r23 (bead 2 -> 3)."""
-    dist12 = math.sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2])
-    dist23 = math.sqrt(r23[0] * r23[0] + r23[1] * r23[1] + r23[2] * r23[2])
-    return np.rad2deg(np.arccos(-(r12[0] * r23[0] + r12[1] * r23[1] + r12[2] * r23[2]) / dist12 / dist23))
-
-
-def pole_distance_pbc(bead1, bead2, bead3, box_size):
-    """bead.py:367-371."""
-    r = pole_pointer_pbc(bead1, bead2, bead3, box_size)
-    return math.sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2])
-
-
 def distance(bead1, bead2):
     r = pointer(bead1, bead2)
     return math.sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2])

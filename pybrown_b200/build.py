@@ -40,7 +40,7 @@ def sources():
 
 def _compile(src, verbose_ptxas):
     obj = os.path.join(OBJ, src[:-3] + ".o")
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-dc" if False else "-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

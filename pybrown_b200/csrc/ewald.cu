@@ -412,23 +412,16 @@ std::map<std::tuple<double, int, int>, EwaldTables*> g_tables;
 
 }  // namespace
 
-int get_ewald_tables(double alpha, int m_max, int n_max, const EwaldTables** out) {
-  if (m_max < 0 || n_max < 0 || m_max > 16 || n_max > 16 || !(alpha > 0)) {
-    pbg_set_error_message("invalid Ewald parameters alpha=%g m_max=%d n_max=%d", alpha, m_max, n_max);
-    return PBG_ERR_ARG;
-  }
-  std::lock_guard<std::mutex> lk(g_tables_mu);
-  auto key = std::make_tuple(alpha, m_max, n_max);
-  auto it = g_tables.find(key);
-  if (it != g_tables.end()) {
-    *out = it->second;
-    return PBG_OK;
-  }
-  auto* t = new EwaldTables();
-  t->alpha = alpha;
-  t->m_max = m_max;
-  t->n_max = n_max;
-  std::vector<double> real, recip;
+long long lattice_points_l1(int m) {
+  // integer points with |x| + |y| + |z| <= m: (2m + 1)(2m^2 + 2m + 3) / 3
+  const long long mm = m;
+  return (2 * mm + 1) * (2 * mm * mm + 2 * mm + 3) / 3;
+}
+
+void build_lattice_tables(double alpha, int m_max, int n_max, std::vector<double>& real,
+                          std::vector<double>& recip, double self_O[6], double self_Q[6]) {
+  real.clear();
+  recip.clear();
   for (int mx = -m_max; mx <= m_max; ++mx)
     for (int my = -(m_max - std::abs(mx)); my <= m_max - std::abs(mx); ++my)
       for (int mz = -(m_max - std::abs(mx) - std::abs(my)); mz <= m_max - std::abs(mx) - std::abs(my); ++mz) {
@@ -449,9 +442,29 @@ int get_ewald_tables(double alpha, int m_max, int n_max, const EwaldTables** out
         const double row[8] = {(double)nx, (double)ny, (double)nz, P, R, S, 0, 0};
         recip.insert(recip.end(), row, row + 8);
       }
+  host_self_sums(alpha, m_max, n_max, self_O, self_Q);
+}
+
+int get_ewald_tables(double alpha, int m_max, int n_max, const EwaldTables** out) {
+  if (m_max < 0 || n_max < 0 || m_max > 16 || n_max > 16 || !(alpha > 0)) {
+    pbg_set_error_message("invalid Ewald parameters alpha=%g m_max=%d n_max=%d", alpha, m_max, n_max);
+    return PBG_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_tables_mu);
+  auto key = std::make_tuple(alpha, m_max, n_max);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    *out = it->second;
+    return PBG_OK;
+  }
+  auto* t = new EwaldTables();
+  t->alpha = alpha;
+  t->m_max = m_max;
+  t->n_max = n_max;
+  std::vector<double> real, recip;
+  build_lattice_tables(alpha, m_max, n_max, real, recip, t->self_O, t->self_Q);
   t->n_real = (int)real.size() / 4;
   t->n_recip = (int)recip.size() / 8;
-  host_self_sums(alpha, m_max, n_max, t->self_O, t->self_Q);
   std::vector<float> recip_f(recip.begin(), recip.end());
   if (cudaMalloc(&t->d_real, real.size() * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&t->d_recip, std::max<size_t>(recip.size(), 8) * sizeof(double)) != cudaSuccess ||

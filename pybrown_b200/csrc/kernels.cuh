@@ -86,6 +86,16 @@ struct EwaldTables {
 
 // Returns the (cached) tables for a parameter set; they live until exit.
 int get_ewald_tables(double alpha, int m_max, int n_max, const EwaldTables** out);
+// Number of integer points with |x| + |y| + |z| <= m: the real-space images
+// of ewald_real = m; (lattice_points_l1(n) - 1) / 2 reciprocal half-vectors
+// of ewald_imag = n.
+long long lattice_points_l1(int m);
+// Host tables of one (alpha, m_max, n_max) set in the layout of EwaldTables
+// (real: 4 doubles per image, recip: 8 doubles per half-vector) and the
+// a-independent self-block lattice sums.  The one builder behind every
+// device copy of the tables.
+void build_lattice_tables(double alpha, int m_max, int n_max, std::vector<double>& real,
+                          std::vector<double>& recip, double self_O[6], double self_Q[6]);
 
 // Writes scale * M for the free-space (smith == false) or Smith-Ewald RPY
 // tensor of positions `pos` into M (row-major, leading dimension ld).

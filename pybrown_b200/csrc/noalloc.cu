@@ -9,6 +9,7 @@
 // computation with every byte of scratch in one file-scope device array of
 // fixed size, so it never allocates.  Every GPU that loads the library holds
 // this array until the process exits.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
@@ -58,68 +59,33 @@ int scratch_address(void** out) {
   return PBG_OK;
 }
 
-// Lattice tables of (alpha, m_max, n_max) in the layout of the Ewald tile
-// kernel: images (mx, my, mz, 0) in the L1-ball loop order of the reference
-// (src/bdsim/clib/diff_tensor.c:675-683), half of the n vectors with weights
-// (nx, ny, nz, P, R, S, 0, 0) doubled for the -n partner, and the
-// a-independent lattice sums of the self block (diff_tensor.c:652-849).
-void host_tables(double alpha, int m_max, int n_max, std::vector<double>& real, std::vector<double>& recip,
-                 double self_O[6], double self_Q[6]) {
-  for (int mx = -m_max; mx <= m_max; ++mx)
-    for (int my = -(m_max - std::abs(mx)); my <= m_max - std::abs(mx); ++my)
-      for (int mz = -(m_max - std::abs(mx) - std::abs(my)); mz <= m_max - std::abs(mx) - std::abs(my); ++mz) {
-        const double v[4] = {(double)mx, (double)my, (double)mz, 0.0};
-        real.insert(real.end(), v, v + 4);
-      }
-  const double kk = PBG_PI * PBG_PI / (alpha * alpha);
-  for (int nx = -n_max; nx <= n_max; ++nx)
-    for (int ny = -(n_max - std::abs(nx)); ny <= n_max - std::abs(nx); ++ny)
-      for (int nz = -(n_max - std::abs(nx) - std::abs(ny)); nz <= n_max - std::abs(nx) - std::abs(ny); ++nz) {
-        if (!(nx > 0 || (nx == 0 && ny > 0) || (nx == 0 && ny == 0 && nz > 0))) continue;
-        const double nl2 = nx * nx + ny * ny + nz * nz;
-        const double e = std::exp(-kk * nl2);
-        const double P = 2.0 * (2.0 / PBG_PI) / nl2 * e;
-        const double R = P * (1.0 + kk * nl2) / nl2;
-        const double S = 2.0 * 4 * PBG_PI * e / nl2;
-        const double v[8] = {(double)nx, (double)ny, (double)nz, P, R, S, 0.0, 0.0};
-        recip.insert(recip.end(), v, v + 8);
-      }
-  // self-block lattice sums, a-independent part
-  const double sqrt_pi = std::sqrt(PBG_PI), alpha2 = alpha * alpha, alpha3 = alpha * alpha2;
-  for (int c = 0; c < 6; ++c) self_O[c] = self_Q[c] = 0.0;
-  for (size_t q = 0; q < real.size(); q += 4) {
-    const double mx = real[q], my = real[q + 1], mz = real[q + 2];
-    if (mx == 0 && my == 0 && mz == 0) continue;
-    const double mm[6] = {mx * mx, my * my, mz * mz, mx * my, mx * mz, my * mz};
-    const double l2 = mm[0] + mm[1] + mm[2], l = std::sqrt(l2), l3 = l2 * l, l5 = l3 * l2;
-    const double ec = std::erfc(alpha * l), e = std::exp(-alpha2 * l2);
-    const double o_fn[6] = {(1 + mm[0] / l2) / l, (1 + mm[1] / l2) / l, (1 + mm[2] / l2) / l,
-                            mm[3] / l3, mm[4] / l3, mm[5] / l3};
-    const double q_fn[6] = {(1 - 3 * mm[0] / l2) / l3, (1 - 3 * mm[1] / l2) / l3, (1 - 3 * mm[2] / l2) / l3,
-                            -3 * mm[3] / l5, -3 * mm[4] / l5, -3 * mm[5] / l5};
-    const double w_o = 2 * alpha / sqrt_pi * e / l2;
-    const double am = alpha * l;
-    const double w_q1 = std::erfc(am) + 2 / sqrt_pi * am * e;
-    const double w_q2 = 2 / sqrt_pi * 2 * alpha3 * e / l2;
-    for (int c = 0; c < 6; ++c) {
-      self_O[c] += ec * o_fn[c] + w_o * mm[c];
-      self_Q[c] += w_q1 * q_fn[c] - w_q2 * mm[c];
-    }
+// Host-to-device copy through kernel parameters: the launch itself carries
+// the values, so nothing is staged in pageable memory and the host does not
+// wait for the stream.  Each launch moves up to TABLE_CHUNK doubles (within
+// the 4 KB classic parameter limit); `dst_f`, if set, also receives them
+// rounded to float.
+constexpr int TABLE_CHUNK = 480;
+struct TableChunk {
+  double v[TABLE_CHUNK];
+  int count;
+};
+
+__global__ void fill_table_kernel(TableChunk c, double* dst, float* dst_f) {
+  for (int t = threadIdx.x; t < c.count; t += blockDim.x) {
+    dst[t] = c.v[t];
+    if (dst_f) dst_f[t] = (float)c.v[t];
   }
-  for (int nx = -n_max; nx <= n_max; ++nx)
-    for (int ny = -(n_max - std::abs(nx)); ny <= n_max - std::abs(nx); ++ny)
-      for (int nz = -(n_max - std::abs(nx) - std::abs(ny)); nz <= n_max - std::abs(nx) - std::abs(ny); ++nz) {
-        if (!nx && !ny && !nz) continue;
-        const double nl2 = nx * nx + ny * ny + nz * nz;
-        const double mm[6] = {(double)nx * nx, (double)ny * ny, (double)nz * nz,
-                              (double)nx * ny, (double)nx * nz, (double)ny * nz};
-        const double w = 2.0 / PBG_PI / nl2 * std::exp(-kk * nl2);
-        const double t = 1.0 / nl2 + kk;
-        for (int c = 0; c < 3; ++c) self_O[c] += w * (1.0 - t * mm[c]);
-        for (int c = 3; c < 6; ++c) self_O[c] += w * (-t * mm[c]);
-        const double wq = 4 * PBG_PI * std::exp(-kk * nl2) / nl2;
-        for (int c = 0; c < 6; ++c) self_Q[c] += wq * mm[c];
-      }
+}
+
+int upload_table(const std::vector<double>& src, double* dst, float* dst_f, cudaStream_t st) {
+  TableChunk c;
+  for (size_t off = 0; off < src.size(); off += TABLE_CHUNK) {
+    c.count = (int)std::min<size_t>(TABLE_CHUNK, src.size() - off);
+    std::copy(src.begin() + off, src.begin() + off + c.count, c.v);
+    fill_table_kernel<<<1, 128, 0, st>>>(c, dst + off, dst_f ? dst_f + off : nullptr);
+    PBG_CHECK_LAUNCH();
+  }
+  return PBG_OK;
 }
 
 }  // namespace
@@ -134,41 +100,44 @@ extern "C" int pbg_dev_smith_matrix_noalloc(const double* pos, const double* rad
     pbg_set_error_message("pbg_dev_smith_matrix_noalloc: invalid arguments");
     return PBG_ERR_ARG;
   }
+  // Sizes are checked from the closed-form lattice counts before any table
+  // is built, so an oversized ewald_real / ewald_imag is refused at once.
+  // (Beyond 64 the counts exceed both capacities anyway.)
+  const long long n_real = m_max > 64 ? (1LL << 40) : lattice_points_l1(m_max);
+  const long long n_recip = n_max > 64 ? (1LL << 40) : (lattice_points_l1(n_max) - 1) / 2;
+  const size_t elem = precision == PBG_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const long double phase_bytes = (long double)n_beads * (long double)n_recip * (long double)elem;
+  if (n_real > NOALLOC_MAX_REAL || n_recip > NOALLOC_MAX_RECIP || phase_bytes > (long double)NOALLOC_PHASE_BYTES) {
+    pbg_set_error_message(
+        "pbg_dev_smith_matrix_noalloc: size beyond the fixed scratch (%lld images of max %d, %lld reciprocal "
+        "vectors of max %d, %.0Lf phase bytes of max %zu)",
+        n_real, NOALLOC_MAX_REAL, n_recip, NOALLOC_MAX_RECIP, phase_bytes, NOALLOC_PHASE_BYTES);
+    return PBG_ERR_ARG;
+  }
   if (n_beads == 0) return PBG_OK;
   cudaStream_t st = (cudaStream_t)stream;
+  void* base = nullptr;
+  int rc = scratch_address(&base);
+  if (rc) return rc;
   std::vector<double> real, recip;
   EwaldTables t;
-  host_tables(alpha, m_max, n_max, real, recip, t.self_O, t.self_Q);
+  build_lattice_tables(alpha, m_max, n_max, real, recip, t.self_O, t.self_Q);
   t.alpha = alpha;
   t.m_max = m_max;
   t.n_max = n_max;
   t.n_real = (int)(real.size() / 4);
   t.n_recip = (int)(recip.size() / 8);
-  const size_t elem = precision == PBG_PREC_FP64 ? sizeof(double2) : sizeof(float2);
-  const size_t phase_bytes = (size_t)n_beads * t.n_recip * elem;
-  if (t.n_real > NOALLOC_MAX_REAL || t.n_recip > NOALLOC_MAX_RECIP || phase_bytes > NOALLOC_PHASE_BYTES) {
-    pbg_set_error_message(
-        "pbg_dev_smith_matrix_noalloc: size beyond the fixed scratch (%d images of max %d, %d reciprocal "
-        "vectors of max %d, %zu phase bytes of max %zu)",
-        t.n_real, NOALLOC_MAX_REAL, t.n_recip, NOALLOC_MAX_RECIP, phase_bytes, NOALLOC_PHASE_BYTES);
-    return PBG_ERR_ARG;
-  }
-  void* base = nullptr;
-  int rc = scratch_address(&base);
-  if (rc) return rc;
   unsigned char* b = static_cast<unsigned char*>(base);
   t.d_real = reinterpret_cast<double*>(b);
   t.d_recip = reinterpret_cast<double*>(b + NOALLOC_REAL_BYTES);
   t.d_recip_f = reinterpret_cast<float*>(b + NOALLOC_REAL_BYTES + NOALLOC_RECIP_BYTES);
   void* phase = b + NOALLOC_REAL_BYTES + NOALLOC_RECIP_BYTES + NOALLOC_RECIP_F_BYTES;
-  std::vector<float> recip_f(recip.begin(), recip.end());
-  // Pageable host sources: the copies are staged before the calls return, so
-  // the local vectors may go out of scope afterwards.
-  PBG_CUDA_TRY(cudaMemcpyAsync(t.d_real, real.data(), real.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  if (!recip.empty()) {
-    PBG_CUDA_TRY(cudaMemcpyAsync(t.d_recip, recip.data(), recip.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    PBG_CUDA_TRY(cudaMemcpyAsync(t.d_recip_f, recip_f.data(), recip_f.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-  }
+  // The tables are rewritten by every call (stream-ordered before the kernels
+  // that read them); the phase tables are fully written by the phase kernel.
+  rc = upload_table(real, t.d_real, nullptr, st);
+  if (rc) return rc;
+  rc = upload_table(recip, t.d_recip, t.d_recip_f, st);
+  if (rc) return rc;
   PairSource src{pos, nullptr, n_beads, box_length};
   return launch_rpy_tensor(src, pos, radii, true, &t, scale, precision, M, ld, phase, st);
 }

@@ -20,7 +20,6 @@ import sys
 import numpy as np
 
 from . import _lib
-from .bead import angle_pbc
 
 
 def kcal_per_mole_to_joule(value):
@@ -50,108 +49,6 @@ def to_joule(F, energy_unit):
     if energy_unit == "eV":
         return eV_to_joule(F)
     return F
-
-
-# ---- pair and triple terms on the host (interactions.py:641-819) ----------
-# The device evaluates these terms for the simulation (csrc/forces.cu); the
-# host functions keep the reference module's API for user code, with the
-# reference's arithmetic order so that results agree bit for bit.
-
-def _dist2_from_pointer(pointer):
-    """interactions.py:847-849."""
-    return pointer[0] * pointer[0] + pointer[1] * pointer[1] + pointer[2] * pointer[2]
-
-
-def _lj_terms(bead1, bead2, pointer):
-    """sigma = sum of the hard-core radii, epsilon = geometric mean of the
-    well depths; returns (epsilon, dist2, (sigma / dist)^2)."""
-    sigma = bead1.hard_core_radius + bead2.hard_core_radius
-    epsilon = math.sqrt(bead1.epsilon_LJ * bead2.epsilon_LJ)
-    dist2 = _dist2_from_pointer(pointer)
-    return epsilon, dist2, sigma * sigma / dist2
-
-
-def harmonic_bond_force(bead1, bead2, pointer):
-    """interactions.py:641-651: k (d - d_eq) along the unit vector of `pointer`."""
-    dist_eq, k = bead1.bonded_how[bead2.bead_id]
-    dist = math.sqrt(_dist2_from_pointer(pointer))
-    return pointer / dist * k * (dist - dist_eq)
-
-
-def harmonic_bond_energy(bead1, bead2, pointer):
-    """interactions.py:655-663: k (d - d_eq)^2 / 2."""
-    dist_eq, k = bead1.bonded_how[bead2.bead_id]
-    dist = math.sqrt(_dist2_from_pointer(pointer))
-    return 0.5 * k * (dist - dist_eq) ** 2
-
-
-def harmonic_angle_force(bead1, bead2, bead3, pointer12, pointer23, box_length):
-    """interactions.py:667-693: forces on the three beads (9 values) of the
-    harmonic angle term k (theta - theta_eq)^2 / 2, angles in radians."""
-    theta_eq, k = bead1.angled_how[(bead2.bead_id, bead3.bead_id)]
-    theta = angle_pbc(pointer12, pointer23)
-    theta_eq *= np.pi / 180.0
-    theta *= np.pi / 180.0
-    d2_12, d2_23 = _dist2_from_pointer(pointer12), _dist2_from_pointer(pointer23)
-    d_12, d_23 = math.sqrt(d2_12), math.sqrt(d2_23)
-    c = np.cos(theta)
-    out = np.zeros(9)
-    out[:3] = (pointer23 / d_23 + c * pointer12 / d_12) / d_12
-    out[3:6] = (pointer12 - pointer23) / d_12 / d_23 - c * (pointer12 / d2_12 - pointer23 / d2_23)
-    out[6:] = -pointer12 / d_12 / d_23 - c * pointer23 / d2_23
-    return k * (theta - theta_eq) / np.sin(theta) * out
-
-
-def harmonic_angle_energy(bead1, bead2, bead3, pointer12, pointer23, box_length):
-    """interactions.py:697-707."""
-    theta_eq, k = bead1.angled_how[(bead2.bead_id, bead3.bead_id)]
-    theta = angle_pbc(pointer12, pointer23)
-    theta_eq *= np.pi / 180.0
-    theta *= np.pi / 180.0
-    return 0.5 * k * (theta - theta_eq) ** 2
-
-
-def LJ_6_attractive_force(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:711-727."""
-    epsilon, dist2, s2 = _lj_terms(bead1, bead2, pointer)
-    dist = math.sqrt(dist2)
-    s6 = s2 * s2 * s2
-    return 6.0 * lennard_jones_alpha * epsilon * s6 / dist * (pointer / dist)
-
-
-def LJ_6_attractive_energy(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:731-743."""
-    epsilon, _, s2 = _lj_terms(bead1, bead2, pointer)
-    return -lennard_jones_alpha * epsilon * (s2 * s2 * s2)
-
-
-def LJ_12_repulsive_force(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:747-763."""
-    epsilon, dist2, s2 = _lj_terms(bead1, bead2, pointer)
-    dist = math.sqrt(dist2)
-    s12 = s2 * s2 * s2 * s2 * s2 * s2
-    return -12.0 * lennard_jones_alpha * epsilon * s12 / dist * (pointer / dist)
-
-
-def LJ_12_repulsive_energy(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:767-779."""
-    epsilon, _, s2 = _lj_terms(bead1, bead2, pointer)
-    return lennard_jones_alpha * epsilon * (s2 * s2 * s2 * s2 * s2 * s2)
-
-
-def LJ_6_12_energy(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:783-797."""
-    epsilon, _, s2 = _lj_terms(bead1, bead2, pointer)
-    s6 = s2 * s2 * s2
-    return lennard_jones_alpha * epsilon * (s6 * s6 - s6)
-
-
-def LJ_6_12_force(bead1, bead2, pointer, lennard_jones_alpha):
-    """interactions.py:801-819."""
-    epsilon, dist2, s2 = _lj_terms(bead1, bead2, pointer)
-    dist = math.sqrt(dist2)
-    s6 = s2 * s2 * s2
-    return lennard_jones_alpha * epsilon / dist * (6 * s6 - 12 * (s6 * s6)) * (pointer / dist)
 
 
 def _index_by_id(beads):
@@ -328,29 +225,6 @@ def set_custom_interactions(input_data):
         how_many_body = int(key.split("_")[-2][:-1])
         out.append(Interactions(getattr(module, force[key]), getattr(module, energy[key]), aux,
                                 bonded=bonded, how_many_body=how_many_body))
-    return out
-
-
-def set_interactions(input_data, beads):
-    """interactions.py:483-513: the host Interactions of a simulation, in the
-    reference's order -- Lennard-Jones (6, 12 or 6-12, when switched on),
-    harmonic bonds and harmonic angles (when any bead has one), then the
-    custom ones.  The device path (DeviceInteractions) evaluates the built-in
-    terms itself; this list serves user code and host-side checks."""
-    out = []
-    lj6, lj12 = bool(input_data["lennard_jones_6"]), bool(input_data["lennard_jones_12"])
-    if lj6 or lj12:
-        pair = {(True, True): (LJ_6_12_force, LJ_6_12_energy),
-                (True, False): (LJ_6_attractive_force, LJ_6_attractive_energy),
-                (False, True): (LJ_12_repulsive_force, LJ_12_repulsive_energy)}[(lj6, lj12)]
-        out.append(Interactions(*pair, {"lennard_jones_alpha": input_data["lennard_jones_alpha"]}, bonded=False,
-                                how_many_body=2))
-    if any(len(b.bonded_with) > 0 for b in beads):
-        out.append(Interactions(harmonic_bond_force, harmonic_bond_energy, {}, bonded=True, how_many_body=2))
-    if any(len(b.angled_with) > 0 for b in beads):
-        out.append(Interactions(harmonic_angle_force, harmonic_angle_energy, {"box_length": input_data["box_length"]},
-                                bonded=True, how_many_body=3))
-    out.extend(set_custom_interactions(input_data))
     return out
 
 

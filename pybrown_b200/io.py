@@ -1,7 +1,4 @@
 """Input and output formats (drop-in for pyBrown.input / pyBrown.output).
-The concentration and flux writers keep the reference's formats; the
-simulations that measure concentration and flux are outside this library
-(Box raises NotImplementedError for those keywords).
 
 JSON configuration with defaults and keyword validation
 (src/bdsim/pyBrown/input.py:24-109), `.str` structure files
@@ -9,7 +6,6 @@ JSON configuration with defaults and keyword validation
 restart files with a `.rst2` backup (output.py:72-84).  Byte formats are the
 reference's.
 """
-import functools
 import json
 import os
 import pickle
@@ -84,17 +80,6 @@ def timestamp(message, *variables):
     print("{}: ".format(date) + message.format(*variables) + "\n")
 
 
-def timing(f):
-    """output.py:32-40: decorator printing how long each call of f took."""
-    @functools.wraps(f)
-    def wrap(*args, **kwargs):
-        t0 = time.time()
-        ret = f(*args, **kwargs)
-        print("{:s} function took {:.3f} ms".format(f.__name__, (time.time() - t0) * 1000.0))
-        return ret
-    return wrap
-
-
 def write_to_xyz_file(xyz_file, xyz_filename, j, dt, beads):
     """output.py:63-69."""
     xyz_file.write("{}\n".format(len(beads)))
@@ -144,23 +129,3 @@ def write_to_enr_file(enr_file, j, dt, E, energy_unit_string):
     if j == 0:
         enr_file.write("time/ps energy/{}\n".format(energy_unit_string))
     enr_file.write("{} {}\n".format(j * dt, E))
-
-
-def _write_labelled_row(f, j, dt, values):
-    """Step 0 writes the header `time/ps <label> ...`; later steps write
-    `<time> <value> ...` in the labels' order (output.py:88-104, 122-138)."""
-    labels = list(values.keys())
-    if j == 0:
-        f.write(("time/ps" + " {}" * len(labels) + "\n").format(*labels))
-    else:
-        f.write(("{}" + " {}" * len(values) + "\n").format(j * dt, *[values[k] for k in labels]))
-
-
-def write_to_con_file(con_file, j, dt, concentration):
-    """output.py:88-104 (concentration per label)."""
-    _write_labelled_row(con_file, j, dt, concentration)
-
-
-def write_to_flux_file(flux_file, j, dt, net_flux):
-    """output.py:122-138 (net flux per label)."""
-    _write_labelled_row(flux_file, j, dt, net_flux)

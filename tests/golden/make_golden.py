@@ -33,7 +33,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_BDSIM = "/root/reference/src/bdsim"
+# root of the reference checkout; PYBROWN_REFERENCE overrides the default
+REFERENCE_BDSIM = os.path.join(os.environ.get("PYBROWN_REFERENCE", "/root/reference"), "src", "bdsim")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libpyBrown.so")
 
 

@@ -6,8 +6,7 @@ Run in a container that has the reference tree and oracle/_ref built:
 
 Seeded beads in a periodic box (some pairs straddling the box edge) go
 through the reference's pure-Python bead functions (src/bdsim/pyBrown/
-bead.py: pointer, pole_pointer, pointer_pbc, pole_pointer_pbc, angle_pbc,
-distance, distance_pbc, pole_distance_pbc, overlap, overlap_pbc,
+bead.py: pointer, pointer_pbc, distance, distance_pbc, overlap, overlap_pbc,
 build_connection_matrix, get_bead_with_id, Bead.translate, Bead.keep_in_box)
 and the results are stored as JSON; tests/test_bead_golden.py only reads it.
 """
@@ -47,7 +46,7 @@ def main():
 
     bs = make()
     out = {"L": L, "pos": pos.tolist(), "radii": radii.tolist(), "bonds": [[1, 3], [3, 5]], "immobile": [7, 8]}
-    pairs, triples = [], []
+    pairs = []
     for i in range(8):
         for j in range(8):
             if i == j:
@@ -60,16 +59,7 @@ def main():
                           "overlap": bool(bead_mod.overlap(bs[i], bs[j])),
                           "overlap_pbc": bool(bead_mod.overlap_pbc(bs[i], bs[j], L)),
                           "overlap_pbc_eps": bool(bead_mod.overlap_pbc(bs[i], bs[j], L, 25.0))})
-    for (i, j, k) in ((0, 1, 2), (2, 3, 4), (5, 4, 3), (1, 0, 6)):
-        r12 = bead_mod.pointer_pbc(bs[i], bs[j], L)
-        r23 = bead_mod.pointer_pbc(bs[j], bs[k], L)
-        triples.append({"i": i, "j": j, "k": k,
-                        "pole_pointer": bead_mod.pole_pointer(bs[i], bs[j], bs[k]).tolist(),
-                        "pole_pointer_pbc": bead_mod.pole_pointer_pbc(bs[i], bs[j], bs[k], L).tolist(),
-                        "pole_distance_pbc": bead_mod.pole_distance_pbc(bs[i], bs[j], bs[k], L),
-                        "angle_pbc": float(bead_mod.angle_pbc(r12, r23))})
     out["pairs"] = pairs
-    out["triples"] = triples
     out["connection_matrix"] = np.asarray(bead_mod.build_connection_matrix(bs)).astype(int).tolist()
     out["get_bead_with_id"] = [bead_mod.get_bead_with_id(bs, k) for k in (1, 5, 8, 99)]
     moved = make()

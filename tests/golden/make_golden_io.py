@@ -7,8 +7,7 @@ Run in a container that has the reference tree and oracle/_ref built:
 It feeds a structure file written here (beads with labels and ids, bonds,
 angles) to the reference's `read_str_file` (src/bdsim/pyBrown/input.py:113-172)
 and records every parsed field; writes two `.xyz` frames and two `.enr`
-lines with the reference's writers (output.py:63-69, 108-118), concentration
-and flux rows (output.py:88-104, 122-138); truncates a
+lines with the reference's writers (output.py:63-69, 108-118); truncates a
 file with `truncate_output_file_during_restart` (output.py:44-60); and
 completes a JSON configuration with `InputData` (input.py:24-109).  The GPU
 box has none of the reference: tests/test_io_golden.py only reads io.json.
@@ -33,7 +32,6 @@ angle 0 2 3 7 1.5 3.0
 """
 
 DEFAULTS = {"T": 298.15, "seed": None, "dt": 1.0}
-LABELLED_ROWS = [{"A": 0, "B": 0}, {"A": 3, "B": -1.5}, {"A": 2.25, "B": 7}]
 REQUIRED = ["box_length"]
 ALL = ["box_length", "T", "seed", "dt", "hydrodynamics"]
 CONFIG = {"box_length": 75.0, "hydrodynamics": "rpy"}
@@ -68,12 +66,6 @@ def main():
             ref_output.write_to_enr_file(f, 0, 0.5, 1.5e-20, "joule")
             ref_output.write_to_enr_file(f, 1, 0.5, -2.25e-21, "joule")
         out["enr_text"] = open(enr).read()
-        for kind, writer in (("con", ref_output.write_to_con_file), ("flux", ref_output.write_to_flux_file)):
-            path = os.path.join(d, kind)
-            with open(path, "w") as f:
-                for j, vals in enumerate(LABELLED_ROWS):
-                    writer(f, j, 0.25, vals)
-            out[kind + "_text"] = open(path).read()
         ref_output.truncate_output_file_during_restart(xyz, 3)
         out["truncated_xyz_text"] = open(xyz).read()
         cfg = os.path.join(d, "c.json")

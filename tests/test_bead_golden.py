@@ -42,17 +42,6 @@ def test_pair_functions(golden):
         assert bool(B.overlap_pbc(b1, b2, L, 25.0)) == p["overlap_pbc_eps"]
 
 
-def test_pole_and_angle_functions(golden):
-    bs, L = _beads(golden), golden["L"]
-    for t in golden["triples"]:
-        b1, b2, b3 = bs[t["i"]], bs[t["j"]], bs[t["k"]]
-        assert B.pole_pointer(b1, b2, b3).tolist() == t["pole_pointer"]
-        assert B.pole_pointer_pbc(b1, b2, b3, L).tolist() == t["pole_pointer_pbc"]
-        assert B.pole_distance_pbc(b1, b2, b3, L) == t["pole_distance_pbc"]
-        r12, r23 = B.pointer_pbc(b1, b2, L), B.pointer_pbc(b2, b3, L)
-        assert float(B.angle_pbc(r12, r23)) == t["angle_pbc"]
-
-
 def test_connection_matrix_ids_and_wrapping(golden):
     bs, L = _beads(golden), golden["L"]
     assert B.build_connection_matrix(bs).tolist() == golden["connection_matrix"]

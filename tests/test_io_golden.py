@@ -62,23 +62,3 @@ def test_input_data_defaults(golden, tmp_path):
     cfg.write_text(json.dumps(golden["config"]))
     inp = io.InputData(str(cfg), golden["required"], golden["defaults"], golden["all_keywords"])
     assert inp.input_data == golden["input_data"]
-
-
-def test_concentration_and_flux_rows(golden, tmp_path):
-    rows = [{"A": 0, "B": 0}, {"A": 3, "B": -1.5}, {"A": 2.25, "B": 7}]
-    for kind, writer in (("con", io.write_to_con_file), ("flux", io.write_to_flux_file)):
-        path = tmp_path / kind
-        with open(path, "w") as f:
-            for j, vals in enumerate(rows):
-                writer(f, j, 0.25, vals)
-        assert path.read_text() == golden[kind + "_text"]
-
-
-def test_timing_decorator(capsys):
-    @io.timing
-    def work(x, y=2):
-        return x * y
-
-    assert work(3, y=4) == 12
-    out = capsys.readouterr().out
-    assert out.startswith("work function took ") and out.rstrip().endswith(" ms")

@@ -6,16 +6,17 @@ not run into the device-wide synchronisation of cudaMalloc/cudaFree.  Its
 scratch is one fixed array inside the library, shared by every call.
 
 Checked through the C ABI against the allocating entry point
-(pbg_dev_smith_matrix) on the same inputs, on two calls in a row (the second
-call finds the first call's data in the shared array), at the tolerance of
-the other FP64 tensor tests.  This file is collected last on purpose.
+(pbg_dev_smith_matrix) on the same inputs, on calls in a row whose lattice
+sizes differ (a larger call, then a smaller one, then a larger one again), so
+stale tables left in the shared array by the previous call would show.  Both
+entry points run the same kernels on the same tables, so the outputs must be
+identical bit for bit.  This file is collected last on purpose.
 """
 import math
 
 import numpy as np
 import pytest
 
-pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 
@@ -41,17 +42,18 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-def test_noalloc_matches_allocating_entry_point_twice():
+@pytest.mark.gpu
+def test_noalloc_matches_allocating_entry_point_in_a_row():
     import torch
     from pybrown_b200 import _lib
     n_beads, L = 300, 900.0
-    alpha, m_max, n_max = math.sqrt(math.pi), 2, 4
+    alpha = math.sqrt(math.pi)
     n = 3 * n_beads
-    cases = [_config(11, n_beads, L, 10.0, 40.0), _config(12, n_beads, L, 10.0, 40.0)]
-    # FP64 at the FP64 tensor tolerance; the mixed (FP32) output at the FP32
-    # level the mixed-precision tests use
-    for prec, dtype, tol in ((0, torch.float64, TOL), (1, torch.float32, 1e-6)):
-        for pos, radii in cases:  # two calls in a row, different inputs
+    # (config seed, ewald_real, ewald_imag): larger, smaller, larger again
+    calls = [(11, 2, 4), (12, 1, 2), (13, 3, 5)]
+    for prec, dtype in ((0, torch.float64), (1, torch.float32)):
+        for seed, m_max, n_max in calls:
+            pos, radii = _config(seed, n_beads, L, 10.0, 40.0)
             dpos = torch.tensor(pos.reshape(-1), dtype=torch.float64, device="cuda")
             drad = torch.tensor(radii, dtype=torch.float64, device="cuda")
             ref = torch.zeros(n * n, dtype=dtype, device="cuda")
@@ -61,12 +63,13 @@ def test_noalloc_matches_allocating_entry_point_twice():
             _lib.call("pbg_dev_smith_matrix_noalloc", dpos.data_ptr(), drad.data_ptr(), n_beads, L, alpha, m_max,
                       n_max, 1.0, prec, out.data_ptr(), n, None)
             torch.cuda.synchronize()
-            r = ref.double().cpu().numpy()
-            o = out.double().cpu().numpy()
+            r = ref.cpu().numpy()
+            o = out.cpu().numpy()
             assert np.all(np.isfinite(o))
-            assert _rel(o, r) <= tol, (prec, _rel(o, r))
+            assert np.array_equal(o, r), (prec, m_max, n_max, _rel(o.astype(np.float64), r.astype(np.float64)))
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_oversized_input():
     import torch
     from pybrown_b200 import _lib
@@ -78,3 +81,21 @@ def test_noalloc_rejects_oversized_input():
                                                2, 4, 1.0, 0, out.data_ptr(), 3 * n_beads, None)
     assert rc == -2  # PBG_ERR_ARG
     assert "fixed scratch" in _lib.last_error()
+
+
+def test_noalloc_rejects_huge_lattice_before_building_tables():
+    """An oversized ewald_real / ewald_imag is refused from the closed-form
+    lattice counts at once, before any table is built or any CUDA call is
+    made (so this runs without a GPU too)."""
+    import ctypes
+    import time
+    from pybrown_b200 import _lib
+    for m_max, n_max in ((1000, 4), (2, 1000), (100000, 100000), (2**31 - 1, 4)):
+        t0 = time.perf_counter()
+        rc = _lib.lib.pbg_dev_smith_matrix_noalloc(ctypes.c_void_p(16), ctypes.c_void_p(16), 64,
+                                                   ctypes.c_double(750.0), ctypes.c_double(math.sqrt(math.pi)),
+                                                   m_max, n_max, ctypes.c_double(1.0), 0, ctypes.c_void_p(16),
+                                                   192, None)
+        assert rc == -2, (m_max, n_max, rc)
+        assert "fixed scratch" in _lib.last_error()
+        assert time.perf_counter() - t0 < 0.5
