@@ -283,6 +283,45 @@ def cpu_reference_steps(N, steps, warmup, threads=None):
     return steps / dt, cores, kind, sample
 
 
+def mixed_vs_oracle(pos, radii, seed, steps=5):
+    """Accuracy of the mixed path against the FP64 oracle (the checker, run
+    outside every timed region): D, B and B xi at the start positions (the
+    first step's matrices and noise) and the displacement after `steps`
+    steps, both fed the same RandomState noise.  Errors are
+    max |a - b| / max |b|."""
+    from oracle.oracle import ORACLE_OMP_LIB, ORACLE_LIB, CLib, OracleBox
+    from pybrown_b200.bead import Bead
+    from pybrown_b200.box import Box
+    lib = CLib(ORACLE_OMP_LIB if os.path.exists(ORACLE_OMP_LIB) else ORACLE_LIB)
+    inp = box_input("mixed")
+    inp["seed"] = seed
+    box = Box([Bead(p.copy(), a) for p, a in zip(pos, radii)], inp)
+    ref_inp = dict(inp)
+    ref_inp.pop("precision")
+    ref = OracleBox(pos, radii, ref_inp, clib=lib)
+    dt, L = WORKLOAD["dt"], WORKLOAD["box_length"]
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    box.propagate(dt)
+    ref.propagate(dt)
+    xi = np.random.RandomState(seed).normal(0.0, 1.0, 3 * len(radii))
+    B = np.tril(box.B)
+    out = {"D": rel(box.D, ref.D), "B": rel(B, ref.B), "Bxi": rel(B @ xi, ref.B @ xi)}
+    for _ in range(steps - 1):
+        box.propagate(dt)
+        ref.propagate(dt)
+    got = np.array([b.r for b in box.beads])
+    dg, dr = got - pos, ref.pos - pos
+    dg -= L * np.round((dg - dr) / L)
+    out["disp"] = rel(dg, dr)
+    out["steps"] = steps
+    out["same_draws"] = bool(box.draw_count == ref.draw_count)
+    out["oracle"] = os.path.basename(lib.path)
+    return out
+
+
 # DRAM bytes (read + write) of one mixed factorisation of the N=1024 matrix,
 # from one ncu capture of the same kernel on the same order:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:chol_df -c 1 --clock-control none \
@@ -373,6 +412,9 @@ def run_ours(args, torch, dist, rank, world):
     value = world * args.steps / (results["mixed"]["ms"] * 1e-3)
     fp64_value = world * args.steps / (results["fp64"]["ms"] * 1e-3)
     cpu = None
+    accuracy = None
+    if world == 1 and not args.no_oracle_check:
+        accuracy = mixed_vs_oracle(pos, radii, seed)
     if world == 1 and not args.no_cpu_baseline:
         sps, cores, kind, sample = cpu_reference_steps(N, steps=2, warmup=1)
         cpu = {"value": sps, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample}
@@ -384,6 +426,7 @@ def run_ours(args, torch, dist, rank, world):
         "config": bench_config(world),
         "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
         "mixed_vs_fp64_displacement_rel_err": rel_err,
+        "mixed_vs_oracle": accuracy,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 8 * 3 * N * 2 + 8 * N, "d2h_bytes_per_step": 8 * 3 * N},
         "gpu_launches": results["mixed"]["launches"],
@@ -553,6 +596,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the mixed-vs-FP64-oracle accuracy check (D, B, B xi, displacement)")
     ap.add_argument("--no-lub", action="store_true", help="skip the lubricated (Stokesian dynamics) section")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replicas section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")

@@ -139,7 +139,8 @@ PBG_API int pbg_dev_check_overlaps(const double *pos, const double *radii, int n
 
 /* In-place lower Cholesky factor of an SPD matrix of order n (row-major,
  * leading dimension ld >= round_up(n, 64), rows/cols n..ld-1 are used as
- * padding).  precision selects FP64 or the mixed FP32 path (float*).
+ * padding).  precision selects FP64, the mixed FP32 path (float*; FP32
+ * diagonal tiles, 3xTF32 trailing updates) or PBG_PREC_MIXED_FP64_DIAG.
  * info_dev (int, device) receives 0 or 1 + the index of the first
  * non-positive pivot. */
 PBG_API int pbg_dev_cholesky(void *A, int n, int ld, int precision, int *info_dev, void *stream);
@@ -156,6 +157,10 @@ PBG_API int pbg_dev_spd_inverse(double *A, int n, int ld, int *info_dev, void *s
 
 #define PBG_PREC_FP64 0
 #define PBG_PREC_MIXED 1
+/* pbg_dev_cholesky only: an FP32 matrix (as PBG_PREC_MIXED) whose 64 x 64
+ * diagonal tiles are factored and inverted in FP64 instead of FP32 (the
+ * factorisation the lubricated mixed path uses for its resistance matrices). */
+#define PBG_PREC_MIXED_FP64_DIAG 2
 
 #define PBG_SCHEME_ERMAK 0
 #define PBG_SCHEME_MIDPOINT 1
@@ -319,7 +324,8 @@ PBG_API int pbg_batch_create(const pbg_params *tmpl, pbg_batch **out);
 PBG_API int pbg_batch_destroy(pbg_batch *b);
 /* Device bytes one replica of n_beads takes (matrices, factor, tables, state). */
 PBG_API long long pbg_batch_footprint(int precision, int hydrodynamics, int ewald_imag, int n_beads);
-/* p: n_beads, box_length, kBT, viscosity, check_overlaps, overlap_treshold.
+/* p: n_beads, box_length, kBT, viscosity, check_overlaps, overlap_treshold,
+ * max_move_attempts (pbg_batch_step; at least 1).
  * pos (3N), radii (N): host or device memory. */
 PBG_API int pbg_batch_add(pbg_batch *b, const pbg_params *p, const double *pos, const double *radii, int *slot);
 PBG_API int pbg_batch_remove(pbg_batch *b, int slot);
@@ -340,6 +346,26 @@ PBG_API int pbg_batch_step_begin(pbg_batch *b, double dt, int build_D, int chole
 PBG_API int pbg_batch_step_attempt(pbg_batch *b, const unsigned char *mask, unsigned char *accepted, void *stream);
 /* status[slot]: 0, the first non-positive pivot (1-based), or -1 (a wait gave up). */
 PBG_API int pbg_batch_step_end(pbg_batch *b, int *status, void *stream);
+/* One whole step of every replica, all of whose noise comes from the
+ * counter-based device streams (pbg_batch_set_seed): the start of the step
+ * (as pbg_batch_step_begin), then rounds of attempts -- each replica still
+ * moving draws 3N normals, moves by sqrt(2 dt) B xi, is tested for overlaps
+ * and, on an overlap, moved back -- until every replica is accepted or has
+ * used max_move_attempts (pbg_params of pbg_batch_add), then the wrap into
+ * the box.  The rounds run on the device under a conditional WHILE node of
+ * the step's CUDA graph (captured once a step repeats with the same
+ * membership, flags and dt; a launch runs at most 4096 rounds, further
+ * rounds are launched from the host), so a repeated step is one graph launch
+ * and one synchronisation.  Each replica's noise, moves and decisions are
+ * those of the attempt-by-attempt path with pbg_batch_fill_noise.
+ * status[slot] as pbg_batch_step_end; attempts[slot] (may be NULL) receives
+ * the attempts each replica took.  PBG_ERR_ATTEMPTS when a replica ran out of
+ * attempts (its last move undone; box.py:248 asserts), then PBG_ERR_BARRIER /
+ * PBG_ERR_NOT_SPD as pbg_batch_step_end.  No counterpart in the reference.
+ * A batch's calls are ordered on the stream they are given: use one stream
+ * per batch. */
+PBG_API int pbg_batch_step(pbg_batch *b, double dt, int build_D, int cholesky, int *status, int *attempts,
+                           void *stream);
 /* D or B (PBG_MAT_D / PBG_MAT_B) of one replica, 3N x 3N FP64 row-major host array. */
 PBG_API int pbg_batch_get_matrix(pbg_batch *b, int slot, int which, double *out);
 
@@ -357,7 +383,8 @@ PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_s
  * time of each candidate, merge order major (8 entries). */
 PBG_API int pbg_batch_autotune(pbg_batch *b, int reps, int *best, float *ms, void *stream);
 /* How the start of a step (Ewald build, copy into B, factorisation,
- * deterministic move) runs: 1 = one CUDA graph launch (captured once a step
+ * deterministic move) -- or with pbg_batch_step the whole step -- runs:
+ * 1 = one CUDA graph launch (captured once a step
  * repeats with the same membership, flags and dt), 0 = its kernels launched
  * one by one, -1 = the driver refused the capture (kernels launched one by
  * one from then on).  No counterpart in the reference. */

@@ -7,6 +7,7 @@ CPU-baseline leg of bench.py, as the checker.  The product never imports it.
 Libraries it can drive (both export the reference's symbols, diff_tensor.c /
 bead.c):
   * oracle/_build/libpybrown_oracle.so -- the in-house C restatement
+  * oracle/_build/libpybrown_oracle_omp.so -- the same on all host cores
   * oracle/_ref/libpyBrown.so          -- the reference's own C compiled here
   * oracle/_ref/libpyBrown_omp.so      -- the same with OpenMP
 """
@@ -18,6 +19,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libpybrown_oracle.so")
+ORACLE_OMP_LIB = os.path.join(HERE, "_build", "libpybrown_oracle_omp.so")
 REF_LIB = os.path.join(HERE, "_ref", "libpyBrown.so")
 REF_OMP_LIB = os.path.join(HERE, "_ref", "libpyBrown_omp.so")
 

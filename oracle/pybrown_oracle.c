@@ -179,6 +179,7 @@ static void orc_rpy_pair(double ai, double aj, double rx, double ry, double rz, 
 void RPY_M_matrix(double *as, double *pointers, int number_of_beads, double *M_matrix)
 {
 	int N = number_of_beads, n3 = 3 * N;
+#pragma omp parallel for schedule(dynamic, 8)
 	for (int j = 0; j < N; j++) {
 		double self = 1.0 / (6 * ORC_PI * as[j]);
 		M_matrix[3 * j + 3 * j * n3] = self;
@@ -390,6 +391,10 @@ void RPY_Smith_M_matrix(double *as, double *pointers, double box_length, double 
                         int n_max, int number_of_beads, double *M_matrix)
 {
 	int N = number_of_beads, n3 = 3 * N;
+	/* Every (i, j) writes its own two blocks: the columns j are independent.
+	 * With -fopenmp (the _omp build) they run on all host cores; the result
+	 * is identical to the serial build. */
+#pragma omp parallel for schedule(dynamic, 4)
 	for (int j = 0; j < N; j++) {
 		double b[6];
 		orc_smith_self_block(as[j], box_length, alpha, m_max, n_max, b);

@@ -73,6 +73,7 @@ class ReplicaBatch:
         p.viscosity = float(viscosity)
         p.check_overlaps = int(bool(check_overlaps))
         p.overlap_treshold = float(overlap_treshold)
+        p.max_move_attempts = max(1, int(max_move_attempts))
         slot = ctypes.c_int(-1)
         _lib.call("pbg_batch_add", self._h, ctypes.byref(p), pos.ctypes.data, rad.ctypes.data, ctypes.byref(slot))
         s = slot.value
@@ -154,11 +155,32 @@ class ReplicaBatch:
         return int(_lib.lib.pbg_batch_graph_state(self._h))
 
     # ---------------------------------------------------------------- step
-    def propagate(self, dt, build_D=True, cholesky=True):
-        """One step of every replica (box.py:150-250, Ermak scheme)."""
+    def propagate(self, dt, build_D=True, cholesky=True, device_loop=None):
+        """One step of every replica (box.py:150-250, Ermak scheme).  When
+        every replica draws device noise the whole step -- attempts included
+        -- runs on the device (pbg_batch_step: one CUDA graph launch once the
+        step repeats); otherwise the attempts are driven from the host, which
+        draws the RandomState noise in the reference's order.  device_loop=False
+        drives the attempts from the host for device noise too (same results)."""
         if not self._rep:
             return
         h, st = self._h, self._stream
+        all_device = all(rec["noise"] == "device" for rec in self._rep.values())
+        if device_loop and not all_device:
+            raise ValueError("the device loop needs device noise for every replica")
+        if all_device and device_loop is not False:
+            ns = _lib.lib.pbg_batch_slots(h)
+            status = np.zeros(ns, dtype=np.int32)
+            attempts = np.zeros(ns, dtype=np.int32)
+            rc = _lib.lib.pbg_batch_step(h, float(dt), int(bool(build_D)), int(bool(cholesky)),
+                                         status.ctypes.data, attempts.ctypes.data, st)
+            for s, rec in self._rep.items():
+                rec["last_move_attempts"] = int(attempts[s])
+            if rc == _lib.PBG_ERR_ATTEMPTS:
+                exceeded = [s for s, rec in self._rep.items() if attempts[s] >= rec["max_move_attempts"]]
+                raise AssertionError("maximal number of move attepts exceeded (slots {})".format(exceeded))
+            _lib.check("pbg_batch_step", rc)
+            return
         _lib.call("pbg_batch_step_begin", h, float(dt), int(bool(build_D)), int(bool(cholesky)), st)
         ns = _lib.lib.pbg_batch_slots(h)
         mask = np.zeros(ns, dtype=np.uint8)

@@ -137,6 +137,17 @@ struct pbg_batch {
   double key_dt = 0;
   int key_repeats = 0;                 // steps in a row with the current key
   bool graph_refused = false;          // the driver refused the capture: direct launches
+  // Whole steps on the device (pbg_batch_step): the start, the rounds of
+  // attempts under a conditional WHILE node and the wrap, as one graph.
+  cudaStream_t cap_stream2 = nullptr;  // captures the loop body
+  cudaGraphExec_t step_exec = nullptr;
+  long long step_fixed_kernels = 0;    // kernels of one replay besides the rounds
+  int* d_att = nullptr;                // [R] attempts of this step (inside d_flags)
+  int* d_words = nullptr;              // [4]: any replica still moving, error bits, rounds, 0
+  int* d_maxatt = nullptr;             // [cap] max_move_attempts per replica
+  int* h_step = nullptr;               // pinned: infos, attempts, words of the last step
+  bool streams_on_device = false;      // d_stream holds every replica's (seed, draws)
+  bool host_draws_stale = false;       // ... and the host copies are behind it
 };
 
 namespace pbg {
@@ -293,6 +304,54 @@ __global__ void batch_noise_kernel(const BatchDev* __restrict__ reps, const unsi
   }
 }
 
+// Start of the attempt rounds of a device step: every replica moves; the
+// attempt counts and the step words are cleared.
+__global__ void batch_round_init_kernel(int R, unsigned char* __restrict__ mask, int* __restrict__ att,
+                                        int* __restrict__ words) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < R; q += gridDim.x * blockDim.x) {
+    mask[q] = 1;
+    att[q] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 4) words[threadIdx.x] = 0;
+}
+
+// End of one round of attempts (one block): each moving replica has taken one
+// more attempt and consumed 3N draws (rounded up to even) of its stream; it
+// stops when its move was accepted (already undone otherwise) or when it has
+// used max_move_attempts (error bit ATTEMPTS, as box.py:248 asserts).
+// words[0] = whether any replica still moves; inside the step's graph the
+// WHILE node's condition is set to it, and a round cap bounds every launch.
+constexpr int BATCH_ROUND_CAP = 4096;
+__global__ void batch_round_update_kernel(const BatchDev* __restrict__ reps, int R, unsigned char* __restrict__ mask,
+                                          const int* __restrict__ ovl, int* __restrict__ att,
+                                          const int* __restrict__ maxatt, unsigned long long* __restrict__ streams,
+                                          int* __restrict__ words, cudaGraphConditionalHandle handle,
+                                          int use_handle) {
+  int moving = 0;
+  for (int q = threadIdx.x; q < R; q += blockDim.x) {
+    if (!mask[q]) continue;
+    const int n = reps[q].n;
+    const int a = att[q] + 1;
+    att[q] = a;
+    streams[2 * q + 1] += (unsigned long long)(n + (n & 1));
+    if (!ovl[q]) {
+      mask[q] = 0;
+    } else if (a >= maxatt[q]) {
+      mask[q] = 0;
+      atomicOr(words + 1, (int)PBG_DEV_ERR_ATTEMPTS);
+    } else {
+      moving = 1;
+    }
+  }
+  const int any = __syncthreads_or(moving);
+  if (threadIdx.x == 0) {
+    const int rounds = words[2] + 1;
+    words[2] = rounds;
+    words[0] = any;
+    if (use_handle) cudaGraphSetConditional(handle, (any && rounds % BATCH_ROUND_CAP != 0) ? 1u : 0u);
+  }
+}
+
 inline size_t elem_size(int precision) { return precision == PBG_PREC_FP64 ? 8 : 4; }
 
 // Replica buffers come from the stream-ordered pool on the legacy default
@@ -360,14 +419,61 @@ __global__ void ewald_work_kernel(const int4* __restrict__ parts, int4* __restri
   }
 }
 
-// Rebuilds the device descriptors and work lists of the current membership:
-// small per-replica descriptors from the host, the task and tile work lists
-// assembled on the device from each replica's cached list.
-int rebuild(pbg_batch* b, cudaStream_t st) {
+// After device steps the device streams are ahead of the host's draw
+// counts: copy them back (active order) before anything reads or changes
+// them on the host or reorders the replicas.
+int pull_draws(pbg_batch* b) {
+  if (!b->host_draws_stale) return PBG_OK;
+  const int R = (int)b->active.size();
+  std::vector<unsigned long long> h(2 * (size_t)R);
+  if (R) PBG_CUDA_TRY(cudaMemcpy(h.data(), b->d_stream, h.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost));
+  for (int q = 0; q < R; ++q) {
+    BatchReplica* r = b->slots[b->active[q]];
+    if (r) r->draws = h[2 * q + 1];
+  }
+  b->host_draws_stale = false;
+  b->streams_on_device = false;
+  return PBG_OK;
+}
+
+// Uploads every replica's (seed, draws) in the active order, unless the
+// device copy is current.
+int push_streams(pbg_batch* b, cudaStream_t st) {
+  if (b->streams_on_device) return PBG_OK;
+  const int R = (int)b->active.size();
+  std::vector<unsigned long long> streams(2 * (size_t)R);
+  for (int q = 0; q < R; ++q) {
+    const BatchReplica* r = b->slots[b->active[q]];
+    streams[2 * q] = r->seed;
+    streams[2 * q + 1] = r->draws;
+  }
+  // pageable source: staged before the call returns
+  if (R) PBG_CUDA_TRY(cudaMemcpyAsync(b->d_stream, streams.data(), streams.size() * sizeof(unsigned long long),
+                                      cudaMemcpyHostToDevice, st));
+  b->streams_on_device = true;
+  return PBG_OK;
+}
+
+void drop_graphs(pbg_batch* b) {
   if (b->begin_exec) {
     cudaGraphExecDestroy(b->begin_exec);
     b->begin_exec = nullptr;
   }
+  if (b->step_exec) {
+    cudaGraphExecDestroy(b->step_exec);
+    b->step_exec = nullptr;
+  }
+}
+
+// Rebuilds the device descriptors and work lists of the current membership:
+// small per-replica descriptors from the host, the task and tile work lists
+// assembled on the device from each replica's cached list.
+int rebuild(pbg_batch* b, cudaStream_t st) {
+  int rc0 = pull_draws(b);
+  if (rc0) return rc0;
+  b->streams_on_device = false;
+  drop_graphs(b);
   b->key_repeats = 0;
   b->key_build = -1;
   b->active.clear();
@@ -376,19 +482,28 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
   const int R = (int)b->active.size();
   b->n_ework = b->ntasks = 0;
   if ((size_t)R > b->cap || !b->d_ovl) {
-    PBG_CUDA_TRY(cudaDeviceSynchronize());
-    free_dev(b->d_ovl);
-    free_dev(b->d_mask);
-    free_dev(b->d_stream);
+    // the kernels of earlier steps on this stream may still read the old
+    // arrays: the stream-ordered frees wait for them, the host buffers are
+    // released once the stream has drained
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    for (void* p : {(void*)b->d_ovl, (void*)b->d_mask, (void*)b->d_stream, (void*)b->d_maxatt})
+      if (p) PBG_CUDA_TRY(cudaFreeAsync(p, st));
+    b->d_ovl = nullptr;
+    b->d_mask = nullptr;
+    b->d_stream = nullptr;
+    b->d_maxatt = nullptr;
     if (b->h_ovl) cudaFreeHost(b->h_ovl);
     if (b->h_info) cudaFreeHost(b->h_info);
-    b->h_ovl = b->h_info = nullptr;
+    if (b->h_step) cudaFreeHost(b->h_step);
+    b->h_ovl = b->h_info = b->h_step = nullptr;
     b->cap = std::max<size_t>(2 * R, 16);
-    PBG_CUDA_TRY(cudaMalloc(&b->d_ovl, b->cap * sizeof(int)));
-    PBG_CUDA_TRY(cudaMalloc(&b->d_mask, b->cap));
-    PBG_CUDA_TRY(cudaMalloc(&b->d_stream, 2 * b->cap * sizeof(unsigned long long)));
+    PBG_CUDA_TRY(cudaMallocAsync((void**)&b->d_ovl, b->cap * sizeof(int), st));
+    PBG_CUDA_TRY(cudaMallocAsync((void**)&b->d_mask, b->cap, st));
+    PBG_CUDA_TRY(cudaMallocAsync((void**)&b->d_stream, 2 * b->cap * sizeof(unsigned long long), st));
+    PBG_CUDA_TRY(cudaMallocAsync((void**)&b->d_maxatt, b->cap * sizeof(int), st));
     PBG_CUDA_TRY(cudaMallocHost(&b->h_ovl, b->cap * sizeof(int)));
     PBG_CUDA_TRY(cudaMallocHost(&b->h_info, b->cap * sizeof(int)));
+    PBG_CUDA_TRY(cudaMallocHost(&b->h_step, (2 * b->cap + 4) * sizeof(int)));
   }
   b->max_n = 0;
   if (R == 0) {
@@ -414,12 +529,16 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
     ntasks += r->seg_start.empty() ? 0 : r->seg_start.back();
     max_seg = std::max(max_seg, (int)r->seg_start.size() - 1);
   }
+  // after the per-replica flags: the infos, the attempt counts and the step
+  // words, contiguous so that one copy reports a step
   const size_t info_off = flag_ints;
-  flag_ints += R;
+  flag_ints += 2 * (size_t)R + 4;
   b->flag_ints = flag_ints;
   int rc;
   if ((rc = ensure(b->d_flags, b->cap_flags, flag_ints * sizeof(int)))) return rc;
   b->d_info = b->d_flags + info_off;
+  b->d_att = b->d_info + R;
+  b->d_words = b->d_att + R;
   std::vector<CholRep> chol(R);
   const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
   for (int q = 0; q < R; ++q) {
@@ -499,6 +618,9 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
   PBG_CUDA_TRY(cudaMemcpyAsync(b->d_rpy, rpy.data(), rpy.size(), cudaMemcpyHostToDevice, st));
   PBG_CUDA_TRY(cudaMemcpyAsync(b->d_chol, chol.data(), R * sizeof(CholRep), cudaMemcpyHostToDevice, st));
   PBG_CUDA_TRY(cudaMemcpyAsync(b->d_eparts, eparts.data(), R * sizeof(int4), cudaMemcpyHostToDevice, st));
+  std::vector<int> maxatt(R);
+  for (int q = 0; q < R; ++q) maxatt[q] = std::max(1, b->slots[b->active[q]]->p.max_move_attempts);
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_maxatt, maxatt.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!segs.empty()) {
     PBG_CUDA_TRY(cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(GatherSeg), cudaMemcpyHostToDevice,
                                  st));
@@ -586,10 +708,13 @@ PBG_API int pbg_batch_destroy(pbg_batch* b) {
   free_dev(b->d_ovl);
   free_dev(b->d_mask);
   free_dev(b->d_stream);
+  free_dev(b->d_maxatt);
   if (b->h_ovl) cudaFreeHost(b->h_ovl);
   if (b->h_info) cudaFreeHost(b->h_info);
-  if (b->begin_exec) cudaGraphExecDestroy(b->begin_exec);
+  if (b->h_step) cudaFreeHost(b->h_step);
+  drop_graphs(b);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->cap_stream2) cudaStreamDestroy(b->cap_stream2);
   delete b;
   return PBG_OK;
 }
@@ -617,6 +742,8 @@ PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, 
     pbg_set_error_message("pbg_batch_add inside a step");
     return PBG_ERR_STATE;
   }
+  int prc = pull_draws(b);
+  if (prc) return prc;
   auto* r = new BatchReplica();
   r->p = *p;
   r->N = p->n_beads;
@@ -673,6 +800,8 @@ PBG_API int pbg_batch_remove(pbg_batch* b, int slot) {
     pbg_set_error_message("pbg_batch_remove inside a step");
     return PBG_ERR_STATE;
   }
+  int rc = pull_draws(b);
+  if (rc) return rc;
   free_replica(r);
   b->slots[slot] = nullptr;
   b->dirty = true;
@@ -716,14 +845,19 @@ PBG_API int pbg_batch_set_noise(pbg_batch* b, int slot, const double* xi) {
 PBG_API int pbg_batch_set_seed(pbg_batch* b, int slot, unsigned long long seed, unsigned long long draws) {
   BatchReplica* r = slot_of(b, slot);
   if (!r) return PBG_ERR_ARG;
+  int rc = pull_draws(b);
+  if (rc) return rc;
   r->seed = seed;
   r->draws = draws + (draws & 1);
+  b->streams_on_device = false;
   return PBG_OK;
 }
 
 PBG_API int pbg_batch_get_draws(pbg_batch* b, int slot, unsigned long long* draws) {
   BatchReplica* r = slot_of(b, slot);
   if (!r || !draws) return PBG_ERR_ARG;
+  int rc = pull_draws(b);
+  if (rc) return rc;
   *draws = r->draws;
   return PBG_OK;
 }
@@ -740,15 +874,10 @@ PBG_API int pbg_batch_fill_noise(pbg_batch* b, const unsigned char* mask, void* 
   int count = 0;
   if ((rc = upload_mask(b, mask, st, &count))) return rc;
   if (!count) return PBG_OK;
-  // the stream positions of this fill (pageable staging, see upload_mask)
-  std::vector<unsigned long long> streams(2 * R);
-  for (int q = 0; q < R; ++q) {
-    const BatchReplica* r = b->slots[b->active[q]];
-    streams[2 * q] = r->seed;
-    streams[2 * q + 1] = r->draws;
-  }
-  PBG_CUDA_TRY(cudaMemcpyAsync(b->d_stream, streams.data(), streams.size() * sizeof(unsigned long long),
-                               cudaMemcpyHostToDevice, st));
+  // the stream positions of this fill (the host counts are authoritative here)
+  if ((rc = pull_draws(b))) return rc;
+  b->streams_on_device = false;
+  if ((rc = push_streams(b, st))) return rc;
   batch_noise_kernel<<<rows_grid(b, 512), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_stream);
   PBG_CHECK_LAUNCH();
   for (int q = 0; q < R; ++q)
@@ -756,6 +885,7 @@ PBG_API int pbg_batch_fill_noise(pbg_batch* b, const unsigned char* mask, void* 
       BatchReplica* r = b->slots[b->active[q]];
       r->draws += (unsigned long long)(r->n + (r->n & 1));
     }
+  b->streams_on_device = false;  // the device copy is now behind the host counts
   return PBG_OK;
 }
 
@@ -869,11 +999,205 @@ PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int chole
   return PBG_OK;
 }
 
-// 1 while the start of a step replays a CUDA graph, 0 while it launches its
-// kernels directly, -1 if the driver refused the capture.
+// One round of attempts of the replicas still moving (mask): their noise,
+// U = B xi, the move, the overlap test, the undo of the rejected moves and
+// the round's bookkeeping (batch_round_update_kernel).  Six kernels.
+static int enqueue_round(pbg_batch* b, cudaStream_t st, cudaGraphConditionalHandle handle, int use_handle) {
+  const int R = (int)b->active.size();
+  const bool f64 = b->precision == PBG_PREC_FP64;
+  const double s1 = std::sqrt(2 * b->dt);
+  batch_noise_kernel<<<rows_grid(b, 512), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_stream);
+  PBG_CHECK_LAUNCH();
+  if (f64) batch_trmv_kernel<double><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, b->d_mask);
+  else batch_trmv_kernel<float><<<rows_grid(b, 8), 256, 0, st>>>(b->d_reps, b->d_mask);
+  PBG_CHECK_LAUNCH();
+  batch_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl, s1, 1.0, 0);
+  PBG_CHECK_LAUNCH();
+  PBG_CUDA_TRY(cudaMemsetAsync(b->d_ovl, 0, R * sizeof(int), st));
+  batch_overlap_kernel<<<dim3(64, R), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl);
+  PBG_CHECK_LAUNCH();
+  batch_move_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps, b->d_mask, b->d_ovl, s1, -1.0, 1);
+  PBG_CHECK_LAUNCH();
+  batch_round_update_kernel<<<1, 1024, 0, st>>>(b->d_reps, R, b->d_mask, b->d_ovl, b->d_att, b->d_maxatt,
+                                                 b->d_stream, b->d_words, handle, use_handle);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+constexpr int ROUND_KERNELS = 6;
+
+// The wrap into the box and the step's report (infos, attempts, words) into
+// pinned host memory.
+static int enqueue_step_tail(pbg_batch* b, cudaStream_t st) {
+  const int R = (int)b->active.size();
+  batch_wrap_kernel<<<rows_grid(b, 256), 256, 0, st>>>(b->d_reps);
+  PBG_CHECK_LAUNCH();
+  PBG_CUDA_TRY(cudaMemcpyAsync(b->h_step, b->d_info, (2 * (size_t)R + 4) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  return PBG_OK;
+}
+
+static int enqueue_round_init(pbg_batch* b, cudaStream_t st) {
+  const int R = (int)b->active.size();
+  batch_round_init_kernel<<<(R + 255) / 256, 256, 0, st>>>(R, b->d_mask, b->d_att, b->d_words);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+// Captures a whole device step into b->step_exec: the start (enqueue_begin),
+// the round initialisation, a conditional WHILE node whose body is one round
+// (its last kernel sets the condition), and the tail.  A refusal by the
+// driver leaves graph_refused set (direct launches from then on).
+static int capture_step(pbg_batch* b, double dt, int build_D, int cholesky, bool any_force) {
+  if (!b->cap_stream) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  if (!b->cap_stream2) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream2, cudaStreamNonBlocking));
+  const long long l0 = pbg_launch_count();
+  auto refuse = [&](cudaGraph_t g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    pbg_count_launches(-(pbg_launch_count() - l0));  // nothing ran
+    b->graph_refused = true;
+    return PBG_OK;
+  };
+  if (cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return refuse(nullptr);
+  int rc = enqueue_begin(b, dt, build_D, cholesky, any_force, b->cap_stream);
+  if (rc == PBG_OK) rc = enqueue_round_init(b, b->cap_stream);
+  const long long fixed0 = pbg_launch_count() - l0;
+  bool ok = rc == PBG_OK;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle handle = 0;
+  cudaGraphNodeParams cp = {};
+  if (ok) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ok = cudaStreamGetCaptureInfo(b->cap_stream, &cs, nullptr, &g, &deps, &ndeps) == cudaSuccess &&
+         cs == cudaStreamCaptureStatusActive &&
+         cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t wnode = nullptr;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&wnode, g, deps, ndeps, &cp) == cudaSuccess &&
+           cudaStreamUpdateCaptureDependencies(b->cap_stream, &wnode, 1, cudaStreamSetCaptureDependencies) ==
+               cudaSuccess;
+    }
+    if (ok) {
+      ok = cudaStreamBeginCaptureToGraph(b->cap_stream2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed) == cudaSuccess;
+      if (ok) {
+        rc = enqueue_round(b, b->cap_stream2, handle, 1);
+        cudaGraph_t body = nullptr;
+        ok = cudaStreamEndCapture(b->cap_stream2, &body) == cudaSuccess && rc == PBG_OK;
+      }
+    }
+  }
+  if (ok) ok = enqueue_step_tail(b, b->cap_stream) == PBG_OK;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(b->cap_stream, &graph);
+  if (!ok || end != cudaSuccess || !graph) return refuse(graph);
+  const cudaError_t inst = cudaGraphInstantiate(&b->step_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) {
+    b->step_exec = nullptr;
+    return refuse(nullptr);
+  }
+  // kernels per replay besides the rounds: the start, the initialisation and the wrap
+  b->step_fixed_kernels = fixed0 + 1;
+  pbg_count_launches(-(pbg_launch_count() - l0));  // nothing ran yet
+  return PBG_OK;
+}
+
+// 1 while the start of a step (or, with pbg_batch_step, the whole step)
+// replays a CUDA graph, 0 while it launches its kernels directly, -1 if the
+// driver refused the capture.
 PBG_API int pbg_batch_graph_state(pbg_batch* b) {
   if (!b) return 0;
-  return b->graph_refused ? -1 : (b->begin_exec ? 1 : 0);
+  return b->graph_refused ? -1 : ((b->begin_exec || b->step_exec) ? 1 : 0);
+}
+
+// A whole step of every replica with device noise (see the header).
+PBG_API int pbg_batch_step(pbg_batch* b, double dt, int build_D, int cholesky, int* status, int* attempts,
+                           void* stream) {
+  if (!b || !(dt > 0)) return PBG_ERR_ARG;
+  if (b->in_step) {
+    pbg_set_error_message("pbg_batch_step inside a step");
+    return PBG_ERR_STATE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (b->dirty && (rc = rebuild(b, st))) return rc;
+  const int R = (int)b->active.size();
+  if (!R) return PBG_OK;
+  if ((rc = push_streams(b, st))) return rc;
+  b->dt = dt;
+  bool any_force = false;
+  for (int s : b->active) any_force = any_force || b->slots[s]->has_force;
+  const bool same = b->key_build == build_D && b->key_chol == cholesky && b->key_force == (int)any_force &&
+                    b->key_dt == dt;
+  if (!same) {
+    drop_graphs(b);
+    b->key_build = build_D;
+    b->key_chol = cholesky;
+    b->key_force = (int)any_force;
+    b->key_dt = dt;
+    b->key_repeats = 0;
+  }
+  ++b->key_repeats;
+  if (!b->step_exec && !b->graph_refused && b->key_repeats >= 2 &&
+      (rc = capture_step(b, dt, build_D, cholesky, any_force)))
+    return rc;
+  const int* words = b->h_step + 2 * R;
+  if (b->step_exec) {
+    PBG_CUDA_TRY(cudaGraphLaunch(b->step_exec, st));
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    pbg_count_launches(b->step_fixed_kernels + (long long)ROUND_KERNELS * words[2]);
+  } else {
+    if ((rc = enqueue_begin(b, dt, build_D, cholesky, any_force, st)) || (rc = enqueue_round_init(b, st)))
+      return rc;
+  }
+  // rounds launched from the host: all of them without a graph, or those
+  // beyond the graph's round cap
+  int* h_words = b->h_step + 2 * R;
+  bool more = !b->step_exec;
+  if (b->step_exec && words[0]) {
+    more = true;
+  }
+  while (more) {
+    if ((rc = enqueue_round(b, st, 0, 0))) return rc;
+    PBG_CUDA_TRY(cudaMemcpyAsync(h_words, b->d_words, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    more = h_words[0] != 0;
+  }
+  if (!b->step_exec || words[0]) {
+    // not replayed, or rounds were added: the tail runs here
+    if ((rc = enqueue_step_tail(b, st))) return rc;
+    PBG_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  b->have_D = b->have_D || build_D;
+  b->streams_on_device = true;
+  b->host_draws_stale = true;
+  int worst = 0;
+  for (int q = 0; q < R; ++q) {
+    const int slot = b->active[q];
+    if (status) status[slot] = b->h_step[q];
+    if (attempts) attempts[slot] = b->h_step[R + q];
+    if (b->h_step[q] < 0) worst = -1;
+    else if (b->h_step[q] > 0 && worst == 0) worst = 1;
+  }
+  if (words[1] & PBG_DEV_ERR_ATTEMPTS) {
+    pbg_set_error_message("maximal number of move attempts exceeded in a batched step");
+    return PBG_ERR_ATTEMPTS;
+  }
+  if (worst < 0) {
+    pbg_set_error_message("a device-wide wait in the batched factorisation gave up");
+    return PBG_ERR_BARRIER;
+  }
+  if (worst > 0) {
+    pbg_set_error_message("a replica's diffusion matrix is not positive definite");
+    return PBG_ERR_NOT_SPD;
+  }
+  return PBG_OK;
 }
 
 PBG_API int pbg_batch_step_attempt(pbg_batch* b, const unsigned char* mask, unsigned char* accepted, void* stream) {

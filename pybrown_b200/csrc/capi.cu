@@ -297,7 +297,8 @@ int pbg_dev_check_overlaps(const double* pos, const double* radii, int n_beads, 
 }
 
 int pbg_dev_cholesky(void* A, int n, int ld, int precision, int* info_dev, void* stream) {
-  if (ld % PBG_TILE || n > ld || n < 0 || (precision != PBG_PREC_FP64 && precision != PBG_PREC_MIXED))
+  if (ld % PBG_TILE || n > ld || n < 0 ||
+      (precision != PBG_PREC_FP64 && precision != PBG_PREC_MIXED && precision != PBG_PREC_MIXED_FP64_DIAG))
     return PBG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   int rc = pbg::launch_pad_identity(A, n, ld, precision, st);

@@ -430,8 +430,35 @@ struct WarpTile64 {
   static constexpr int NQ = 2;
 };
 
+// The FP32 counterpart on the FMA pipe (the FP32 chain inverts its diagonal
+// tiles in FP32): lane (g, t) forms D[g][2t], D[g][2t + 1] as K-term dot
+// products in ascending k.
+struct WarpTile32 {
+  static constexpr int TM = 8;
+  static __device__ __forceinline__ void mma(const float* A, int lda, const float* B, int ldb, int K, float d[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float d0 = 0.0f, d1 = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const float4 a4 = *reinterpret_cast<const float4*>(A + g * lda + k0);
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float2 b = *reinterpret_cast<const float2*>(B + (k0 + q) * ldb + 2 * t);
+        d0 = fmaf(av[q], b.x, d0);
+        d1 = fmaf(av[q], b.y, d1);
+      }
+    }
+    d[0] = d0;
+    d[1] = d1;
+  }
+  static __device__ __forceinline__ int row(int q) { return (threadIdx.x & 31) >> 2; }
+  static __device__ __forceinline__ int col(int q) { return 2 * (threadIdx.x & 3) + (q & 1); }
+  static constexpr int NQ = 2;
+};
+
 template <typename T> struct WarpTileOf;
 template <> struct WarpTileOf<double> { using type = WarpTile64; };
+template <> struct WarpTileOf<float> { using type = WarpTile32; };
 
 // Inverse of the lower-triangular L_kk (in Lk, [64][LDA], zero above the
 // diagonal) into X ([64][LDA]), with Rinv[j] = 1 / L_jj and scratch Tm
@@ -806,6 +833,232 @@ __device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
     for (int cs = 0; cs < 8; ++cs) s[acc_row(rs) * LDA + acc_col(cs)] = acc[TileMMA<T>::idx(rs, cs)];
 }
 
+// ---------------------------------------------------------------- FP32 chain
+// The mixed path's chain CTA factors, inverts and solves in FP32: the
+// diagonal tiles of a well-conditioned FP32 matrix lose nothing to FP32
+// pivots that FP32 storage and the 3xTF32 updates have not already cost,
+// while every step of the panel chain gets shorter (MUFU rsqrt instead of
+// a refined FP64 rsqrt, FP32 FMA latency, no FP64 conversion).
+
+// Named barriers (0 is __syncthreads): arrive does not wait; both order the
+// calling threads' earlier shared-memory accesses before the barrier completes.
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_wait(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// T[r][c] -= sum_q T[r][c0+q] T[c][c0+q] (q = 0..7, in order): the rank-8
+// update of one trailing element with the factored panel c0..c0+7.
+__device__ __forceinline__ void panel_update(float* T, int r, int c, int c0) {
+  const float4 a0 = *reinterpret_cast<const float4*>(T + r * LDA + c0);
+  const float4 a1 = *reinterpret_cast<const float4*>(T + r * LDA + c0 + 4);
+  const float4 b0 = *reinterpret_cast<const float4*>(T + c * LDA + c0);
+  const float4 b1 = *reinterpret_cast<const float4*>(T + c * LDA + c0 + 4);
+  float v = T[r * LDA + c];
+  v = fmaf(-a0.x, b0.x, v);
+  v = fmaf(-a0.y, b0.y, v);
+  v = fmaf(-a0.z, b0.z, v);
+  v = fmaf(-a0.w, b0.w, v);
+  v = fmaf(-a1.x, b1.x, v);
+  v = fmaf(-a1.y, b1.y, v);
+  v = fmaf(-a1.z, b1.z, v);
+  v = fmaf(-a1.w, b1.w, v);
+  T[r * LDA + c] = v;
+}
+
+// F(k) of the FP32 chain on the tile T (smem [64][LDA]: lower triangle valid
+// with every update applied; the caller's writes end with a CTA barrier).
+// Eight 8-column panels.  Warp 0 factors panel p -- the 8 x 8 pivot block in
+// every lane's registers (the pivot chain is rsqrt -> multiply -> FMA) and
+// the strip rows below it (L_r = A_r L_pp^-T, one row per lane) -- while
+// warps 1-7 apply the rank-8 update of panel p-1 to the trailing lower
+// triangle: first the eight columns of panel p+1 (look-ahead), then the
+// rest.  Named barrier 1: panel p factored (warp 0 arrives, warps 1-7
+// wait); named barrier 2: panel p+1's columns updated (warps 1-7 arrive,
+// warp 0 waits).  The update of panel p's columns (c0..c0+7) by warps 1-7 and
+// warp 0's work on them never overlap, nor do the look-ahead and the rest.
+// Returns after a CTA barrier with L_kk in T's lower triangle (the upper one
+// as it was) and Rinv[j] = 1 / L_jj.  A non-positive (or NaN) pivot is
+// recorded in info.
+__device__ __forceinline__ void factor_tile_f32(const DFArgs& a, int k, float* T, float* Rinv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+#pragma unroll 1
+    for (int p = 0; p < 8; ++p) {
+      const int c0 = 8 * p;
+      if (p > 0) bar_wait(2, THREADS);
+      float l[8][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) lds_vec(T + (c0 + i) * LDA + c0, l[i]);
+      int bad = -1;
+      float rinv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float d = l[j][j];
+        if (!(d > 0.0f) && bad < 0) bad = j;
+        const float rs = rsqrtf(d);
+        rinv[j] = rs;
+        l[j][j] = d * rs;
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i) l[i][j] *= rs;
+#pragma unroll
+        for (int i = j + 1; i < 8; ++i)
+#pragma unroll
+          for (int c = j + 1; c <= i; ++c) l[i][c] = fmaf(-l[i][j], l[c][j], l[i][c]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = c0 + 8 + lane + 32 * h;
+        if (r < NB) {
+          float x[8];
+          lds_vec(T + r * LDA + c0, x);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            x[j] *= rinv[j];
+#pragma unroll
+            for (int c = j + 1; c < 8; ++c) x[c] = fmaf(-x[j], l[c][j], x[c]);
+          }
+          *reinterpret_cast<float4*>(T + r * LDA + c0) = make_float4(x[0], x[1], x[2], x[3]);
+          *reinterpret_cast<float4*>(T + r * LDA + c0 + 4) = make_float4(x[4], x[5], x[6], x[7]);
+        }
+      }
+      if (lane < 8) {  // lane i writes row c0 + i of the pivot block (zero above the diagonal) and 1 / L_ii
+        float row[8], rv = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) row[c] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (i == lane) {
+#pragma unroll
+            for (int c = 0; c <= i; ++c) row[c] = l[i][c];
+            rv = rinv[i];
+          }
+        *reinterpret_cast<float4*>(T + (c0 + lane) * LDA + c0) = make_float4(row[0], row[1], row[2], row[3]);
+        *reinterpret_cast<float4*>(T + (c0 + lane) * LDA + c0 + 4) = make_float4(row[4], row[5], row[6], row[7]);
+        Rinv[c0 + lane] = rv;
+      }
+      if (lane == 0 && bad >= 0 && k * NB + c0 + bad < a.n) atomicCAS(a.info, 0, k * NB + c0 + bad + 1);
+      bar_arrive(1, THREADS);
+    }
+  } else {
+    const int t = threadIdx.x - 32, nthr = THREADS - 32;
+#pragma unroll 1
+    for (int p = 0; p < 8; ++p) {
+      const int c0 = 8 * p;
+      bar_wait(1, THREADS);
+      if (p == 7) break;
+      // look-ahead: the columns c0+8 .. c0+15 of panel p+1, rows below them
+      for (int e = t; e < (NB - c0 - 8) * 8; e += nthr) {
+        const int r = c0 + 8 + (e >> 3), c = c0 + 8 + (e & 7);
+        if (c <= r) panel_update(T, r, c, c0);
+      }
+      bar_arrive(2, THREADS);
+      // the rest of the trailing triangle: columns >= c0 + 16
+      const int w = NB - c0 - 16;
+      for (int e = t; e < w * w; e += nthr) {
+        const int r = c0 + 16 + e / w, c = c0 + 16 + e % w;
+        if (c <= r) panel_update(T, r, c, c0);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Shared memory of the FP32 chain: five [64][LDA] float tiles (the tile
+// being factored, inv(L_kk), the solve's input, the previous solve's
+// result, the prefetched next diagonal tile), the inversion scratch
+// (32 x 36) and 1 / L_jj.
+constexpr size_t chain_f32_smem_bytes() { return sizeof(float) * (5 * NB * LDA + 32 * 36 + NB); }
+
+// The FP32 chain CTA: for k = 0, 1, ...
+//   A_kk after its updates by the workers, minus L(k,k-1) L(k,k-1)^T (3xTF32
+//   on the tensor cores; L(k,k-1) is still in shared memory);
+//   F(k) (factor_tile_f32), inv(L_kk) (FP32, on the FMA pipe) -- L_kk goes to
+//   the factor and inv(L_kk) to invdiag, published as fin(k,k) = 2 for the
+//   workers' solves (no I(k) tasks in this list);
+//   S(k+1,k) = A(k+1,k) inv(L_kk)^T (3xTF32), kept in shared memory for the
+//   next step and published as fin(k+1,k) = 1.
+// The solve's input is fetched during F(k) when its last update is already
+// done, and the next diagonal tile during S(k+1,k) when its worker updates
+// are.
+__device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
+  __shared__ int s_pf[2];  // [0] next diagonal tile fetched, [1] solve input fetched
+  float* T = reinterpret_cast<float*>(smem);
+  float* X = T + NB * LDA;
+  float* Cn = X + NB * LDA;
+  float* Lp = Cn + NB * LDA;
+  float* sA = Lp + NB * LDA;
+  float* Tm = sA + NB * LDA;
+  float* Rinv = Tm + 32 * 36;
+  const int nt = a.nt;
+  bool pf_diag = false;
+  for (int k = 0; k < nt; ++k) {
+    float acc[16];
+    TRACE(0, a.ntasks + 2 * k);
+    TRACE(3, a.ntasks + 2 * k);
+    if (k > 0) {
+      if (pf_diag) {
+        cp_async_wait_all();
+        __syncthreads();
+        smem_to_acc(sA, acc);
+      } else {
+        if (!wait_geq(a, a.upd + k * nt + k, k - 1, s_ok)) return;
+        load_acc(tile<float>(a, k, k), a.ld, acc);
+      }
+      TileMMA<float>::sub(Lp, Lp, acc);
+    } else {
+      load_acc(tile<float>(a, 0, 0), a.ld, acc);
+    }
+    acc_to_smem(acc, T);
+    if (threadIdx.x == 0) s_pf[1] = k + 1 < nt && ld_acquire(a.upd + (k + 1) * nt + k) >= k;
+    __syncthreads();
+    // thread 0's acquire and the barrier order the early fetch after the updates
+    const bool have_in = s_pf[1] != 0;
+    if (have_in) stage_async(tile<float>(a, k + 1, k), a.ld, Cn, LDA);
+    TRACE(1, a.ntasks + 2 * k);
+    factor_tile_f32(a, k, T, Rinv);
+    invert_factor<float>(T, Rinv, X, Tm);
+    {  // L_kk (zero above the diagonal) and inv(L_kk), 16 bytes per store
+      float* g = tile<float>(a, k, k);
+      float* inv = reinterpret_cast<float*>(a.invdiag) + (size_t)k * NB * NB;
+#pragma unroll
+      for (int q = 0; q < NB * NB / 4 / THREADS; ++q) {
+        const int e = threadIdx.x + q * THREADS, r = e >> 4, c = (e & 15) * 4;
+        float4 v = *reinterpret_cast<const float4*>(T + r * LDA + c);
+        if (c + 1 > r) v.y = 0.0f;
+        if (c + 2 > r) v.z = 0.0f;
+        if (c + 3 > r) v.w = 0.0f;
+        if (c > r) v.x = 0.0f;
+        *reinterpret_cast<float4*>(g + (size_t)r * a.ld + c) = v;
+        *reinterpret_cast<float4*>(inv + r * NB + c) = *reinterpret_cast<const float4*>(X + r * LDA + c);
+      }
+    }
+    publish(a.fin + k * nt + k, 2);
+    TRACE(2, a.ntasks + 2 * k);
+    if (k + 1 == nt) return;
+    TRACE(0, a.ntasks + 2 * k + 1);
+    TRACE(3, a.ntasks + 2 * k + 1);
+    if (!have_in) {
+      if (!wait_geq(a, a.upd + (k + 1) * nt + k, k, s_ok)) return;
+      stage_async(tile<float>(a, k + 1, k), a.ld, Cn, LDA);
+    }
+    if (threadIdx.x == 0) s_pf[0] = ld_acquire(a.upd + (k + 1) * nt + k + 1) >= k;
+    cp_async_wait_all();
+    __syncthreads();
+    pf_diag = s_pf[0] != 0;
+    if (pf_diag) stage_async(tile<float>(a, k + 1, k + 1), a.ld, sA, LDA);
+    TRACE(1, a.ntasks + 2 * k + 1);
+    solve_by_inverse(Cn, X, acc);
+    acc_to_smem(acc, Lp);
+    __syncthreads();
+    store_tile(Lp, LDA, tile<float>(a, k + 1, k), a.ld);
+    publish(a.fin + (k + 1) * nt + k, 1);
+    TRACE(2, a.ntasks + 2 * k + 1);
+  }
+}
+
 // Shared memory of the chain CTA: four T tiles Cp, Cn, X, sA ([64][LDA]
 // each) and the FP64 factor scratch -- in the FP64 path X holds L_kk from F(k)
 // to S(k+1, k); in the mixed path two more FP64 tiles (L_kk, the FP64 rows of
@@ -1001,12 +1254,16 @@ __device__ __forceinline__ void update_tile_triple(const DFArgs& a, int i, int j
   for (int r = 0; r < 3; ++r) store_tile(sC[r], LDA, tile<T>(a, i + r, j), a.ld);
 }
 
-template <typename T>
+// F32CHAIN (FP32 matrices only): the chain CTA runs the FP32 chain
+// (run_chain_f32) and the task list has no I(k) tasks; otherwise run_chain,
+// whose diagonal tiles are factored in FP64.
+template <typename T, bool F32CHAIN>
 __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_task, s_ok;
   if (blockIdx.x == 0) {
-    run_chain<T>(a, smem, &s_ok);
+    if constexpr (F32CHAIN) run_chain_f32(a, smem, &s_ok);
+    else run_chain<T>(a, smem, &s_ok);
     return;
   }
   T* sA = reinterpret_cast<T*>(smem);
@@ -1217,10 +1474,12 @@ std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
 // Task list of the worker CTAs for an nt x nt tile grid (see the file comment).
-// group: updates per task down a column (2, or 3 for the FP32 kernel).
-int get_task_table(int nt, int group, const int4** out, int* count) {
+// group: updates per task down a column (2, or 3 for the FP32 kernel);
+// inv_tasks: the I(k) tasks that invert the diagonal tiles (left out when the
+// chain CTA stores the inverses itself).
+int get_task_table(int nt, int group, bool inv_tasks, const int4** out, int* count) {
   std::lock_guard<std::mutex> lk(g_task_mu);
-  const int key = nt * 4 + group;
+  const int key = (nt * 4 + group) * 2 + (inv_tasks ? 1 : 0);
   auto it = g_task_tables.find(key);
   if (it != g_task_tables.end()) {
     *out = it->second.first;
@@ -1230,12 +1489,12 @@ int get_task_table(int nt, int group, const int4** out, int* count) {
   // The chain tasks F(k) and S(k+1, k) run on the chain CTA and are left out;
   // so is I(nt-1), which the chain forms after its last factorisation.
   std::vector<int4> t;
-  if (nt > 1) t.push_back(make_int4(TASK_I, 0, 0, 0));
+  if (nt > 1 && inv_tasks) t.push_back(make_int4(TASK_I, 0, 0, 0));
   for (int i = 2; i < nt; ++i) t.push_back(make_int4(TASK_S, i, 0, 0));
   for (int k = 0; k + 1 < nt; ++k) {
     // the last update of the chain's S(k+2, k+1), first: it runs during F(k+1)
     if (k + 2 < nt) t.push_back(make_int4(TASK_U, k + 2, k + 1, k));
-    if (k + 2 < nt) t.push_back(make_int4(TASK_I, 0, 0, k + 1));
+    if (k + 2 < nt && inv_tasks) t.push_back(make_int4(TASK_I, 0, 0, k + 1));
     for (int i = k + 3; i < nt; ++i) t.push_back(make_int4(TASK_S, i, k + 1, k + 1));
     // the rest of column k+1 of the update with panel k is fused into F(k+1)
     // and the workers' S(., k+1); the plain updates cover columns >= k+2, the
@@ -1263,16 +1522,18 @@ int get_task_table(int nt, int group, const int4** out, int* count) {
   return PBG_OK;
 }
 
-template <typename T>
+template <typename T, bool F32CHAIN>
 size_t df_smem_bytes() {
   // the chain, or a grouped update (three in FP32, two in FP64)
-  return std::max(chain_smem_bytes<T>(), (sizeof(T) == 4 ? 7 : 5) * NB * LDA * sizeof(T));
+  return std::max(F32CHAIN ? chain_f32_smem_bytes() : chain_smem_bytes<T>(),
+                  (sizeof(T) == 4 ? 7 : 5) * NB * LDA * sizeof(T));
 }
 
 // tasks_override / spin_limit: only for the wait-expiry self-test.
-template <typename T>
+template <typename T, bool F32CHAIN = false>
 int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned* err, cudaStream_t st,
               const int4* tasks_override = nullptr, int ntasks_override = 0, long long spin_limit = SPIN_LIMIT) {
+  static_assert(!F32CHAIN || sizeof(T) == 4, "the FP32 chain factors FP32 matrices");
   const int nt = ld / NB;
   const int4* tasks = nullptr;
   int ntasks = 0;
@@ -1280,18 +1541,20 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
     tasks = tasks_override;
     ntasks = ntasks_override;
   } else {
-    int rc = get_task_table(nt, sizeof(T) == 4 ? 3 : 2, &tasks, &ntasks);
+    int rc = get_task_table(nt, sizeof(T) == 4 ? 3 : 2, !F32CHAIN, &tasks, &ntasks);
     if (rc) return rc;
   }
-  const size_t smem = df_smem_bytes<T>();
+  const size_t smem = df_smem_bytes<T, F32CHAIN>();
   static int max_blocks_per_sm = -1;
   static int num_sms = 0;
   if (max_blocks_per_sm < 0) {
-    PBG_CUDA_TRY(cudaFuncSetAttribute(chol_df_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PBG_CUDA_TRY(cudaFuncSetAttribute(chol_df_kernel<T, F32CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
     int dev;
     PBG_CUDA_TRY(cudaGetDevice(&dev));
     PBG_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-    PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, chol_df_kernel<T>, THREADS, smem));
+    PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, chol_df_kernel<T, F32CHAIN>,
+                                                               THREADS, smem));
     if (max_blocks_per_sm < 1) {
       pbg_set_error_message("cholesky kernel does not fit on an SM");
       return PBG_ERR_CUDA;
@@ -1326,7 +1589,7 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_df_kernel<T>, args));
+  PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_df_kernel<T, F32CHAIN>, args));
   PBG_CHECK_LAUNCH();
   return PBG_OK;
 }
@@ -1347,7 +1610,7 @@ extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(l
   if (spin_limit < 1 || spin_limit > (1LL << 24)) return PBG_ERR_ARG;
   const int4* full = nullptr;
   int nfull = 0;
-  int rc = get_task_table(nt, 2, &full, &nfull);
+  int rc = get_task_table(nt, 2, true, &full, &nfull);
   if (rc) return rc;
   std::vector<int4> tasks(nfull);
   PBG_CUDA_TRY(cudaMemcpy(tasks.data(), full, nfull * sizeof(int4), cudaMemcpyDeviceToHost));
@@ -1438,8 +1701,10 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
   }
   int* ints = static_cast<int*>(work);
   unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 2 * (size_t)nt * nt);
-  return precision == PBG_PREC_FP64 ? launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st)
-                                    : launch_df<float>((float*)A, n, ld, info, invdiag, ints, err, st);
+  if (precision == PBG_PREC_FP64) return launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st);
+  if (precision == PBG_PREC_MIXED_FP64_DIAG)
+    return launch_df<float, false>((float*)A, n, ld, info, invdiag, ints, err, st);
+  return launch_df<float, true>((float*)A, n, ld, info, invdiag, ints, err, st);
 }
 
 
@@ -1823,7 +2088,7 @@ int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st) {
     pbg_set_error_message("tensor-core inverse: misaligned workspace");
     return PBG_ERR_ARG;
   }
-  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED, info, w.invdiag, w.scratch, st);
+  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED_FP64_DIAG, info, w.invdiag, w.scratch, st);
   if (rc != PBG_OK) return rc;
   return trtri_tc<float>(w.F, w.invdiag, w.X, ld, st);
 }

@@ -46,14 +46,16 @@ def main(argv=None):
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--beads", type=int, default=256)
     ap.add_argument("--order", type=int, default=0, help="cholesky: matrix order (default 3 x beads)")
-    ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--precision", choices=("fp64", "mixed", "mixed_fp64_diag"), default="mixed",
+                    help="mixed_fp64_diag: cholesky only, the FP32 factorisation with FP64 diagonal tiles")
     ap.add_argument("--reps", type=int, default=2)
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return _batch(a, torch)
     if a.kernel == "lub":
         return _lub(a, torch)
-    prec = _lib.PREC[a.precision]
+    chol_prec = {"fp64": 0, "mixed": 1, "mixed_fp64_diag": 2}[a.precision]
+    prec = min(chol_prec, 1)  # the Ewald build: FP64 or FP32
     dtype = torch.float64 if prec == 0 else torch.float32
     beads = a.order // 3 if a.order else a.beads
     L = 1500.0 * (beads / 1024.0) ** (1.0 / 3.0)  # volume fraction of the N=1024 workload
@@ -76,7 +78,7 @@ def main(argv=None):
 
     def cholesky():
         M.copy_(A0)
-        _lib.call("pbg_dev_cholesky", M.data_ptr(), n, ld, prec, info.data_ptr(), None)
+        _lib.call("pbg_dev_cholesky", M.data_ptr(), n, ld, chol_prec, info.data_ptr(), None)
 
     fn = smith if a.kernel == "smith" else cholesky
     fn()

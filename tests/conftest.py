@@ -25,6 +25,16 @@ def oracle_lib():
 
 
 @pytest.fixture(scope="session")
+def oracle_omp_lib():
+    """The same restatement built with OpenMP (identical results, all host
+    cores): the checker for the full-size configurations."""
+    from oracle import oracle
+    if not os.path.exists(oracle.ORACLE_OMP_LIB):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+    return oracle.CLib(oracle.ORACLE_OMP_LIB)
+
+
+@pytest.fixture(scope="session")
 def tensors():
     return np.load(os.path.join(GOLDEN, "tensors.npz"))
 

@@ -274,3 +274,56 @@ def test_device_noise_is_standard_normal():
     assert abs(np.corrcoef(z[:-1], z[1:])[0, 1]) < 0.05
     assert batch.draws(s) == 4 * 3 * N
     batch.close()
+
+
+def test_device_step_loop_matches_host_driven_attempts():
+    """pbg_batch_step (every attempt round on the device, one CUDA graph per
+    repeated step) gives, bit for bit, the positions, attempt counts and noise
+    stream positions of the attempt-by-attempt path driven from the host,
+    including replicas with rejected moves (dense boxes) and a membership
+    change between steps."""
+    from pybrown_b200.batch import ReplicaBatch
+    configs = [_config(700 + k, N, phi, 10.0, 30.0) for k, (N, phi) in
+               enumerate(((64, 0.05), (150, 0.30), (90, 0.25), (40, 0.05)))]
+
+    def run(device_loop):
+        batch = ReplicaBatch(precision="mixed")
+        slots = [batch.add(p, r, l, seed=70 + k, noise="device") for k, (p, r, l) in enumerate(configs[:3])]
+        out, att, states = [], [], []
+        for step in range(6):
+            if step == 3:
+                slots.append(batch.add(*configs[3], seed=73, noise="device"))
+            batch.propagate(10.0, device_loop=device_loop)  # long steps: rejections in the dense boxes
+            states.append(batch.graph_state())
+            out.append(np.concatenate([batch.positions(s).ravel() for s in slots]))
+            att.append([batch.last_move_attempts(s) for s in slots])
+        draws = [batch.draws(s) for s in slots]
+        batch.close()
+        return out, att, draws, states
+
+    dev = run(True)
+    host = run(False)
+    for a, b in zip(dev[0], host[0]):
+        assert np.array_equal(a, b)
+    assert dev[1] == host[1]
+    assert dev[2] == host[2]
+    assert max(max(a) for a in dev[1]) > 1  # some moves were rejected and redrawn
+    assert dev[3] == [0, 1, 1, 0, 1, 1]  # captured on a repeat, dropped by the membership change
+
+
+def test_device_step_loop_attempt_limit():
+    """A replica that can never be accepted (two beads overlapping at the
+    start) stops after max_move_attempts with every move undone and the
+    step raises, as box.py:248 asserts."""
+    from pybrown_b200.batch import ReplicaBatch
+    pos = np.array([[0.0, 0.0, 0.0], [5.0, 0.0, 0.0], [40.0, 40.0, 40.0]])
+    radii = np.array([10.0, 10.0, 10.0])
+    batch = ReplicaBatch(precision="fp64")
+    s = batch.add(pos, radii, 200.0, seed=3, noise="device", max_move_attempts=5)
+    other = batch.add(*_config(5, 30, 0.05, 10.0, 20.0), seed=4, noise="device")
+    with pytest.raises(AssertionError):
+        batch.propagate(0.01)
+    assert batch.last_move_attempts(s) == 5
+    assert batch.last_move_attempts(other) >= 1
+    assert np.allclose(batch.positions(s), pos, rtol=0, atol=1e-12)
+    batch.close()

@@ -58,9 +58,20 @@ def test_cholesky_not_spd_reports_pivot():
     assert info > 0
 
 
-@pytest.mark.parametrize("n", [192, 768, 3072])
-def test_cholesky_mixed(n):
+# prec 1: FP32 chain (FP32 diagonal tiles); prec 2: FP64 diagonal tiles
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("n", [3, 64, 192, 577, 768, 3072])
+def test_cholesky_mixed(n, prec):
     A = _spd(n, 7, cond=1e2)
-    L, info = _run("chol", A, n, prec=1)
+    L, info = _run("chol", A, n, prec=prec)
     assert info == 0
     assert rel_err(np.tril(L), np.linalg.cholesky(A)) <= 5e-5
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_cholesky_mixed_not_spd_reports_pivot(prec):
+    n = 200
+    A = _spd(n, 5)
+    A[140, 140] = -1.0
+    _, info = _run("chol", A, n, prec=prec)
+    assert info > 0
