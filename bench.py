@@ -399,6 +399,23 @@ def run_ours(args, torch, dist, rank, world):
     e2e_ms = timed_steps(torch, lambda: box.propagate(dt), args.steps, flush)
     e2e_ms = max_over_ranks(torch, dist, e2e_ms)
 
+    # the same with an .xyz frame every step through the drivers' writer thread
+    e2e_xyz_ms = None
+    if world == 1:
+        from pybrown_b200.io import AsyncXYZWriter
+        labels = [b.label for b in box.beads]
+        with tempfile.TemporaryDirectory() as d, open(os.path.join(d, "t.xyz"), "w", buffering=1) as f, \
+                AsyncXYZWriter(f, "t.xyz", labels) as writer:
+            j = [0]
+
+            def step_with_frame():
+                writer.write(j[0], dt, box.positions())
+                box.propagate(dt)
+                j[0] += 1
+
+            e2e_xyz_ms = timed_steps(torch, step_with_frame, args.steps, flush)
+            writer.flush()
+
     # dominant kernel: the Cholesky factorisation of D (3072 x 3072)
     chol_ms, info = cholesky_kernel_timing(torch, results["mixed"]["run"].box, 3)
     n = 3 * N
@@ -429,6 +446,9 @@ def run_ours(args, torch, dist, rank, world):
         "mixed_vs_oracle": accuracy,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 8 * 3 * N * 2 + 8 * N, "d2h_bytes_per_step": 8 * 3 * N},
+        "e2e_with_xyz_every_step": (None if e2e_xyz_ms is None else
+                                    {"value": args.steps / (e2e_xyz_ms * 1e-3), "unit": "steps/s",
+                                     "writer": "drivers' .xyz writer thread, one frame per step"}),
         "gpu_launches": results["mixed"]["launches"],
         "roofline": {"kernel": "cholesky (mixed)", "bound": "tensor", "achieved": achieved_tflops,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
@@ -443,7 +463,8 @@ def run_ours(args, torch, dist, rank, world):
     # A failure in a secondary section is reported in its own key (the
     # exception type and message) instead of costing the whole line.
     sections = (("lubrication", args.no_lub, run_lub_section), ("batch", args.no_batch, run_batch_section),
-                ("serve", args.no_serve, run_serve_section))
+                ("serve", args.no_serve, run_serve_section),
+                ("serve_full_stream", args.no_serve or args.no_serve_full, run_serve_full_section))
     for key, skip, fn in sections:
         if world != 1 or skip:
             continue
@@ -531,14 +552,18 @@ def run_batch_section(args, torch):
     tune = batch.autotune(reps=2)  # schedule of the batched factorisation (results unchanged)
     torch.cuda.synchronize()
     launches0 = _lib.lib.pbg_launch_count()
+    calls0 = _lib.lib.pbg_host_launch_count()
+    attempts = 0
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
     for _ in range(args.steps):
         batch.propagate(0.5)
+        attempts += max(batch.last_move_attempts(s) for s in batch.slots())
     end.record()
     torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     launches = (_lib.lib.pbg_launch_count() - launches0) / args.steps
+    calls = (_lib.lib.pbg_host_launch_count() - calls0) / args.steps
     graph = batch.graph_state()
     beads = int(Ns.sum())
     batch.close()
@@ -547,7 +572,9 @@ def run_batch_section(args, torch):
             "steps": args.steps, "ms_per_step": ms / args.steps,
             "bead_steps_per_s": beads * args.steps / (ms * 1e-3),
             "replica_steps_per_s": 256 * args.steps / (ms * 1e-3), "gpu_launches_per_step": launches,
-            "step_start_graph": {1: "one CUDA graph launch", 0: "direct launches", -1: "capture refused"}[graph],
+            "host_launch_calls_per_step": calls, "attempt_rounds_per_step": attempts / args.steps,
+            "step_graph": {1: "one CUDA graph launch per step (attempt rounds under a device-side WHILE node)",
+                           0: "direct launches", -1: "capture refused"}[graph],
             "schedule": {"merge_order": tune["merge_order"], "ctas_per_sm": tune["ctas_per_sm"],
                          "factorisation_ms": {f"{o}/{c}": round(v, 4) for (o, c), v in tune["ms"].items()}}}
 
@@ -570,6 +597,33 @@ def run_serve_section(args, torch):
     summary["offered_bead_steps_per_s"] = sum(r.n_beads * r.steps for r in stream) / args.serve_seconds
     summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
     summary["peak_gb"] = summary.pop("peak_bytes") / 1e9
+    return summary
+
+
+def run_serve_full_section(args, torch):
+    """The full serving stream: Poisson 50 requests/s for 60 s, N log-uniform
+    in [16, 2048], radii uniform in [10, 40], phi 0.05, steps uniform in
+    [100, 5000], dt 1 ps, mixed precision, device noise; wall clock.  One B200
+    cannot keep up with it (about 5e7 bead-steps/s offered), so the run is
+    cut: admissions end when the stream ends and the loop stops a drain time
+    later; the requests still waiting or running are reported as backlog,
+    latencies are those of the completed requests."""
+    from pybrown_b200.batch import ReplicaBatch
+    from pybrown_b200.serve import Server, make_stream
+    duration = 60.0
+    stream = make_stream(4, rate=50.0, duration=duration, steps_min=100, steps_max=5000, dt=1.0, lazy=True)
+    server = Server(ReplicaBatch(precision="mixed"), keep_positions=False, max_active=args.serve_max_active)
+    recs, summary = server.run(stream, clock="wall", stop_admission_at=duration, drain_limit=args.serve_drain)
+    server.batch.close()
+    summary["workload"] = ("Poisson 50 req/s for 60 s, N log-U[16,2048], a~U[10,40], phi=0.05, steps U[100,5000], "
+                           "dt=1, mixed, device noise; admissions end at 60 s, the loop "
+                           f"{args.serve_drain:g} s later; at most {args.serve_max_active} requests run together")
+    summary["offered_bead_steps_per_s"] = sum(r.n_beads * r.steps for r in stream) / duration
+    summary["completed_bead_steps"] = sum(r.n_beads * r.steps for r in recs if math.isfinite(r.completed))
+    summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
+    summary["peak_gb"] = summary.pop("peak_bytes") / 1e9
+    used = summary.pop("peak_device_used_bytes")
+    summary["peak_device_used_gb"] = None if used is None else used / 1e9
     return summary
 
 
@@ -603,6 +657,11 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving stream")
     ap.add_argument("--serve-steps", type=int, nargs=2, default=(5, 30), help="steps per request: min max")
+    ap.add_argument("--no-serve-full", action="store_true", help="skip the full 60 s serving stream")
+    ap.add_argument("--serve-drain", type=float, default=60.0,
+                    help="full serving stream: seconds the loop runs on after admissions end")
+    ap.add_argument("--serve-max-active", type=int, default=256,
+                    help="full serving stream: requests running together at most")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -53,6 +53,9 @@ PBG_API const char *pbg_last_error(void);
 PBG_API int pbg_version(void);
 /* Number of kernels this library has launched in the process so far. */
 PBG_API long long pbg_launch_count(void);
+/* Launch calls the host has made (each kernel launched directly and each CUDA
+ * graph launch count one; the kernels inside a graph do not). */
+PBG_API long long pbg_host_launch_count(void);
 
 /* ============================================================= Tier 1 ==== */
 /* Reference ABI, drop-in replacements for libpyBrown's exports.            */
@@ -332,6 +335,9 @@ PBG_API int pbg_batch_remove(pbg_batch *b, int slot);
 PBG_API int pbg_batch_slots(pbg_batch *b);
 PBG_API int pbg_batch_set_positions(pbg_batch *b, int slot, const double *pos);
 PBG_API int pbg_batch_get_positions(pbg_batch *b, int slot, double *out);
+/* The same copy ordered on `stream` without waiting for it (out: pinned host
+ * memory for the copy to be asynchronous). */
+PBG_API int pbg_batch_get_positions_async(pbg_batch *b, int slot, double *out, void *stream);
 /* External force (3N), or NULL for none. */
 PBG_API int pbg_batch_set_force(pbg_batch *b, int slot, const double *F);
 /* Noise of the next attempt (3N normals, host or device memory). */

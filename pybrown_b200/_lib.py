@@ -104,6 +104,7 @@ _SIGNATURES = {
     "pbg_last_error": (ctypes.c_char_p, []),
     "pbg_version": (_i, []),
     "pbg_launch_count": (_ll, []),
+    "pbg_host_launch_count": (_ll, []),
     "pbg_dev_pointer_matrix": (_i, [_vp, _i, _d, _vp, _vp]),
     "pbg_dev_rpy_matrix": (_i, [_vp, _vp, _i, _d, _d, _vp, _i, _vp]),
     "pbg_dev_smith_matrix": (_i, [_vp, _vp, _i, _d, _d, _i, _i, _d, _i, _vp, _i, _vp]),
@@ -139,6 +140,7 @@ _SIGNATURES = {
     "pbg_batch_slots": (_i, [_vp]),
     "pbg_batch_set_positions": (_i, [_vp, _i, _vp]),
     "pbg_batch_get_positions": (_i, [_vp, _i, _vp]),
+    "pbg_batch_get_positions_async": (_i, [_vp, _i, _vp, _vp]),
     "pbg_batch_set_force": (_i, [_vp, _i, _vp]),
     "pbg_batch_set_noise": (_i, [_vp, _i, _vp]),
     "pbg_batch_set_seed": (_i, [_vp, _i, ctypes.c_ulonglong, ctypes.c_ulonglong]),

@@ -25,8 +25,8 @@ from contextlib import ExitStack
 
 import numpy as np
 
-from .io import (InputData, read_str_file, timestamp, truncate_output_file_during_restart, write_to_enr_file,
-                 write_to_restart_file, write_to_xyz_file)
+from .io import (AsyncXYZWriter, InputData, read_str_file, timestamp, truncate_output_file_during_restart,
+                 write_to_enr_file, write_to_restart_file)
 
 REQUIRED_KEYWORDS = ["output_xyz_filename", "input_str_filename", "box_length", "T", "viscosity", "dt",
                      "number_of_steps"]
@@ -106,17 +106,53 @@ def run_sequential(inp, jobs):
 
 
 def _loop(box, inp, index, job, xyz, enr, j0, n_steps, dt, n_write, n_diff, n_lub, n_chol, restart, energy):
+    """BD.py:160-186.  The .xyz frames go through a writer thread (the loop
+    hands over a copy of the positions); a restart file waits for the frames
+    written so far, since it records the .xyz file's length."""
     extra = [job["enr"]] if energy else []
-    for j in range(j0, n_steps):
-        if inp["debug"]:
-            print("STEP {}\n".format(j))
-        if j % n_write == 0:
-            write_to_xyz_file(xyz, job["xyz"], j, dt, box.beads)
-        box.propagate(dt, j % n_diff == 0, j % n_lub == 0, j % n_chol == 0)
-        if energy and j % inp["enr_write_freq"] == 0:
-            write_to_enr_file(enr, j, dt, box.E, inp["energy_unit"])
-        if restart and j != 0 and j % inp["rst_write_freq"] == 0:
-            write_to_restart_file(job["rst"], index, j, box, job["xyz"], extra)
+    with AsyncXYZWriter(xyz, job["xyz"], [b.label for b in box.beads]) as writer:
+        for j in range(j0, n_steps):
+            if inp["debug"]:
+                print("STEP {}\n".format(j))
+            if j % n_write == 0:
+                writer.write(j, dt, box.positions())
+            box.propagate(dt, j % n_diff == 0, j % n_lub == 0, j % n_chol == 0)
+            if energy and j % inp["enr_write_freq"] == 0:
+                write_to_enr_file(enr, j, dt, box.E, inp["energy_unit"])
+            if restart and j != 0 and j % inp["rst_write_freq"] == 0:
+                writer.flush()
+                write_to_restart_file(job["rst"], index, j, box, job["xyz"], extra)
+
+
+class _FrameBuffers:
+    """Rings of pinned host buffers for the batched .xyz frames: a frame's
+    positions are copied device-to-host asynchronously (on the batch's
+    stream, so before the next step moves them) and the writer threads wait
+    for an event recorded after the copies.  Each ring has depth + 2 buffers,
+    so a buffer is reused only after its writer has formatted it (a writer
+    holds at most depth pending frames and one being written)."""
+
+    depth = 4
+
+    def __init__(self, sizes):
+        import torch
+        self.torch = torch
+        self.rings = [torch.empty((self.depth + 2, n, 3), dtype=torch.float64, pin_memory=True) for n in sizes]
+        self.k = 0
+
+    def capture(self, batch, slots):
+        from . import _lib
+        k = self.k % (self.depth + 2)
+        self.k += 1
+        bufs = []
+        for ring, s in zip(self.rings, slots):
+            buf = ring[k]
+            _lib.call("pbg_batch_get_positions_async", batch._h, int(s), buf.data_ptr(), batch._stream)
+            bufs.append(buf.numpy())
+        ev = self.torch.cuda.Event()
+        ev.record(self.torch.cuda.current_stream() if batch._stream is None else
+                  self.torch.cuda.ExternalStream(batch._stream))
+        return bufs, ev.synchronize
 
 
 def run_batched(inp, jobs, beads_per_job):
@@ -144,15 +180,18 @@ def run_batched(inp, jobs, beads_per_job):
                       max_move_attempts=inp["max_move_attempts"], force=F if np.any(F != 0) else None)
         slots.append(s)
     start = time.time()
+    frames = _FrameBuffers([len(beads) for beads in beads_per_job])
     with ExitStack() as stack:
         xyz = [stack.enter_context(open(job["xyz"], "w", buffering=1)) for job in jobs]
         enr = [stack.enter_context(open(job["enr"], "w", buffering=1)) for job in jobs] if energy else None
+        writers = [stack.enter_context(AsyncXYZWriter(f, job["xyz"], [b.label for b in beads], frames.depth))
+                   for f, job, beads in zip(xyz, jobs, beads_per_job)]
         for j in range(n_steps):
             if j % n_write == 0:
-                for k, (job, beads, s) in enumerate(zip(jobs, beads_per_job, slots)):
-                    for b, r in zip(beads, batch.positions(s)):
-                        b.r = r.copy()
-                    write_to_xyz_file(xyz[k], job["xyz"], j, dt, beads)
+                # device-to-host copies into pinned buffers, ordered before the next step
+                bufs, ready = frames.capture(batch, slots)
+                for w, buf in zip(writers, bufs):
+                    w.write(j, dt, buf, ready)
             batch.propagate(dt, build_D=j % n_diff == 0, cholesky=j % n_chol == 0)
             if energy and j % inp["enr_write_freq"] == 0:
                 for f in enr:

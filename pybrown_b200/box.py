@@ -291,6 +291,12 @@ class Box:
             _lib.call("pbg_set_positions", self._h, self._pos.ctypes.data, self._stream)
             self._pos_synced[...] = self._pos
 
+    def positions(self):
+        """A copy of every bead's position (bead order, N x 3)."""
+        if not self.immobile_beads:
+            return self._pos.copy()
+        return np.array([b.r for b in self.beads], dtype=np.float64)
+
     def sync_positions_from_beads(self):
         """Re-link Bead.r to the box after a caller replaced a bead's r array."""
         for i, b in enumerate(self.mobile_beads):

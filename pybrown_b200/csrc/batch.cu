@@ -824,6 +824,15 @@ PBG_API int pbg_batch_get_positions(pbg_batch* b, int slot, double* out) {
   return PBG_OK;
 }
 
+// Stream-ordered copy of one replica's positions into `out` (pinned host
+// memory for the copy to be asynchronous); the caller waits on the stream.
+PBG_API int pbg_batch_get_positions_async(pbg_batch* b, int slot, double* out, void* stream) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !out) return PBG_ERR_ARG;
+  PBG_CUDA_TRY(cudaMemcpyAsync(out, r->pos, r->n * sizeof(double), cudaMemcpyDefault, (cudaStream_t)stream));
+  return PBG_OK;
+}
+
 PBG_API int pbg_batch_set_force(pbg_batch* b, int slot, const double* F) {
   BatchReplica* r = slot_of(b, slot);
   if (!r) return PBG_ERR_ARG;
@@ -933,6 +942,7 @@ static int capture_begin(pbg_batch* b, double dt, int build_D, int cholesky, boo
   const cudaError_t end = cudaStreamEndCapture(b->cap_stream, &graph);
   const long long kernels = pbg_launch_count() - l0;
   pbg_count_launches(-kernels);  // nothing ran yet
+  pbg_count_host_calls(-kernels);
   if (rc != PBG_OK || end != cudaSuccess || !graph) {
     if (graph) cudaGraphDestroy(graph);
     cudaGetLastError();
@@ -991,6 +1001,7 @@ PBG_API int pbg_batch_step_begin(pbg_batch* b, double dt, int build_D, int chole
   if (b->begin_exec) {
     PBG_CUDA_TRY(cudaGraphLaunch(b->begin_exec, st));
     pbg_count_launches(b->begin_kernels);
+    pbg_count_host_calls(1);
   } else if ((rc = enqueue_begin(b, dt, build_D, cholesky, any_force, st))) {
     return rc;
   }
@@ -1053,7 +1064,9 @@ static int capture_step(pbg_batch* b, double dt, int build_D, int cholesky, bool
   auto refuse = [&](cudaGraph_t g) {
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
-    pbg_count_launches(-(pbg_launch_count() - l0));  // nothing ran
+    const long long k = pbg_launch_count() - l0;  // nothing ran
+    pbg_count_launches(-k);
+    pbg_count_host_calls(-k);
     b->graph_refused = true;
     return PBG_OK;
   };
@@ -1104,7 +1117,9 @@ static int capture_step(pbg_batch* b, double dt, int build_D, int cholesky, bool
   }
   // kernels per replay besides the rounds: the start, the initialisation and the wrap
   b->step_fixed_kernels = fixed0 + 1;
-  pbg_count_launches(-(pbg_launch_count() - l0));  // nothing ran yet
+  const long long k = pbg_launch_count() - l0;  // nothing ran yet
+  pbg_count_launches(-k);
+  pbg_count_host_calls(-k);
   return PBG_OK;
 }
 
@@ -1152,6 +1167,7 @@ PBG_API int pbg_batch_step(pbg_batch* b, double dt, int build_D, int cholesky, i
     PBG_CUDA_TRY(cudaGraphLaunch(b->step_exec, st));
     PBG_CUDA_TRY(cudaStreamSynchronize(st));
     pbg_count_launches(b->step_fixed_kernels + (long long)ROUND_KERNELS * words[2]);
+    pbg_count_host_calls(1);
   } else {
     if ((rc = enqueue_begin(b, dt, build_D, cholesky, any_force, st)) || (rc = enqueue_round_init(b, st)))
       return rc;

@@ -143,10 +143,15 @@ void pbg_record_cuda_error(cudaError_t e, const char* what, const char* file, in
   g_last_error = buf;
 }
 
-static std::atomic<long long> g_launches{0};
+static std::atomic<long long> g_launches{0};     // kernels run
+static std::atomic<long long> g_host_calls{0};   // launch calls made by the host (kernels and graphs)
 
-void pbg_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void pbg_count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  g_host_calls.fetch_add(1, std::memory_order_relaxed);
+}
 void pbg_count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void pbg_count_host_calls(long long n) { g_host_calls.fetch_add(n, std::memory_order_relaxed); }
 
 void pbg_set_error_message(const char* fmt, ...) {
   char buf[512];
@@ -164,6 +169,8 @@ const char* pbg_last_error(void) { return g_last_error.c_str(); }
 int pbg_version(void) { return 10000; }
 
 long long pbg_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+long long pbg_host_launch_count(void) { return g_host_calls.load(std::memory_order_relaxed); }
 
 // ------------------------------------------------------------------ tier 1
 

@@ -37,6 +37,9 @@ void pbg_count_launch();
 // Adds n launches (kernels replayed inside a CUDA graph; negative to take
 // back the launches a stream capture counted without running them).
 void pbg_count_launches(long long n);
+// Adds n host launch calls (+1 per graph launch; negative to take back the
+// kernel launches a stream capture counted).
+void pbg_count_host_calls(long long n);
 
 // Device-side error bits (written with atomicOr into a status word).
 enum : unsigned {

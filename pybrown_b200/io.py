@@ -88,6 +88,83 @@ def write_to_xyz_file(xyz_file, xyz_filename, j, dt, beads):
         xyz_file.write("{} {} {} {}\n".format(bead.label, *bead.r))
 
 
+def _xyz_frame(xyz_filename, j, dt, labels, positions):
+    """The text of one frame in the format of write_to_xyz_file."""
+    lines = ["{}\n".format(len(labels)), "{} time [ps] {}\n".format(xyz_filename, j * dt)]
+    lines.extend("{} {} {} {}\n".format(label, *r) for label, r in zip(labels, positions))
+    return "".join(lines)
+
+
+class AsyncXYZWriter:
+    """.xyz frames (output.py:63-69) written by a background thread, so that a
+    step loop hands over a frame and goes on.  Each frame is a snapshot of the
+    positions (an array copied at hand-over, or a buffer that an asynchronous
+    device-to-host copy is filling, with `ready` a callable that blocks until
+    the copy is done).  The thread waits for the copy, formats the frame
+    exactly as write_to_xyz_file does and writes frames in order.  At most
+    `depth` frames are pending; flush() waits for all of them (before the
+    file's length is read, e.g. for a restart file) and re-raises an error of
+    the thread; close() waits for them and stops the thread."""
+
+    def __init__(self, xyz_file, xyz_filename, labels, depth=4):
+        import queue
+        import threading
+        self._file = xyz_file
+        self._name = xyz_filename
+        self._labels = list(labels)
+        self._queue = queue.Queue(maxsize=max(1, int(depth)))
+        self._error = None
+        self._thread = threading.Thread(target=self._run, name="xyz-writer", daemon=True)
+        self._thread.start()
+
+    def _run(self):
+        while True:
+            item = self._queue.get()
+            try:
+                if item is None:
+                    return
+                j, dt, positions, ready = item
+                if self._error is None:
+                    if ready is not None:
+                        ready()
+                    self._file.write(_xyz_frame(self._name, j, dt, self._labels, positions))
+            except BaseException as e:  # noqa: BLE001 -- re-raised in the caller's thread
+                self._error = e
+            finally:
+                self._queue.task_done()
+
+    def _check(self):
+        if self._error is not None:
+            err, self._error = self._error, None
+            raise err
+
+    def write(self, j, dt, positions, ready=None):
+        """Queues frame j (time j * dt).  Without `ready` the positions are
+        copied now; with it they are read once ready() has returned."""
+        self._check()
+        pos = np.array(positions, dtype=np.float64, copy=True) if ready is None else positions
+        self._queue.put((j, dt, pos, ready))
+
+    def flush(self):
+        """Waits until every frame handed over is written and flushed to the
+        file (a restart file records the .xyz file's length)."""
+        self._queue.join()
+        self._check()
+        self._file.flush()
+
+    def close(self):
+        if self._thread.is_alive():
+            self._queue.put(None)
+            self._thread.join()
+        self._check()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def _file_length(filename):
     i = -1
     with open(filename, "r") as f:

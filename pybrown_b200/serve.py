@@ -14,8 +14,10 @@ by its seed, so its result does not depend on what else was running: it is
 the same alone and in the mix.
 
 Completion latency = completion time - arrival time.  ``run`` returns the
-per-request records and a summary with p50/p99 latency and the aggregate
-bead-steps/s over the run.
+per-request records and a summary with p50/p99 latency of the completed
+requests, the bead-steps/s the batched steps delivered, and -- when the run
+is cut off (admissions end at ``stop_admission_at``, the loop ``drain_limit``
+seconds later) -- the backlog of requests still waiting or running.
 
 Two clocks: ``"wall"`` (real time; arrivals are released when the wall clock
 reaches them) and ``"virtual"`` (time advances by ``tick`` per batched step
@@ -33,7 +35,7 @@ import numpy as np
 class Request:
     rid: int
     arrival: float          # s since the start of the stream
-    positions: np.ndarray   # N x 3, Angstrom
+    positions: np.ndarray   # N x 3, Angstrom (None: placed on first use, see placement_seed)
     radii: np.ndarray       # N, Angstrom
     box_length: float       # Angstrom
     steps: int
@@ -41,6 +43,18 @@ class Request:
     dt: float = 1.0         # ps
     T: float = 293.15
     viscosity: float = 0.01005
+    placement_seed: int = None  # positions = place_beads_fast(default_rng(placement_seed), radii, box)
+
+    def __post_init__(self):
+        if self.positions is None and self.placement_seed is None:
+            raise ValueError("a request needs positions or a placement seed")
+
+    def materialize(self):
+        """Places the beads now if they were left for first use."""
+        if self.positions is None:
+            self.positions = place_beads_fast(np.random.default_rng(self.placement_seed), self.radii,
+                                              self.box_length)
+        return self.positions
 
     @property
     def n_beads(self):
@@ -63,11 +77,13 @@ class Record:
 
 
 def make_stream(seed, rate, duration, n_min=16, n_max=2048, a_lo=10.0, a_hi=40.0, phi=0.05,
-                steps_min=100, steps_max=5000, dt=1.0):
+                steps_min=100, steps_max=5000, dt=1.0, lazy=False):
     """Poisson arrivals at `rate` per second for `duration` seconds; N
     log-uniform in [n_min, n_max], radii uniform in [a_lo, a_hi], random
     non-overlapping positions in a periodic cubic box at volume fraction phi,
-    step count uniform in [steps_min, steps_max]."""
+    step count uniform in [steps_min, steps_max].  With lazy=True each
+    request's beads are placed when it is first used (admission), from its
+    own seeded generator, so that a long stream costs nothing up front."""
     rng = np.random.default_rng(seed)
     t, out, rid = 0.0, [], 0
     while True:
@@ -77,11 +93,39 @@ def make_stream(seed, rate, duration, n_min=16, n_max=2048, a_lo=10.0, a_hi=40.0
         N = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
         radii = rng.uniform(a_lo, a_hi, size=N)
         L = (np.sum(4.0 / 3.0 * np.pi * radii ** 3) / phi) ** (1.0 / 3.0)
-        pos = place_beads(rng, radii, L)
+        if lazy:
+            pos, pseed = None, int(rng.integers(0, 2 ** 63))
+        else:
+            pos, pseed = place_beads(rng, radii, L), None
         steps = int(rng.integers(steps_min, steps_max + 1))
-        out.append(Request(rid, t, pos, radii, float(L), steps, int(rng.integers(0, 2 ** 63)), dt))
+        out.append(Request(rid, t, pos, radii, float(L), steps, int(rng.integers(0, 2 ** 63)), dt,
+                           placement_seed=pseed))
         rid += 1
     return out
+
+
+def place_beads_fast(rng, radii, L, max_rounds=1000):
+    """Random non-overlapping placement (minimum image) for dilute boxes:
+    every bead drawn uniformly in the box at once, then, round by round, the
+    higher-indexed bead of each overlapping pair (found with a periodic k-d
+    tree) drawn again, until no pair overlaps."""
+    from scipy.spatial import cKDTree
+    N = len(radii)
+    pos = rng.uniform(-L / 2, L / 2, size=(N, 3))
+    reach = 2.0 * float(np.max(radii))
+    for _ in range(max_rounds):
+        tree = cKDTree(np.mod(pos + L / 2, L), boxsize=L)
+        pairs = tree.query_pairs(reach, output_type="ndarray")
+        if len(pairs):
+            d = pos[pairs[:, 0]] - pos[pairs[:, 1]]
+            d -= L * np.round(d / L)
+            hit = np.einsum("ij,ij->i", d, d) <= (radii[pairs[:, 0]] + radii[pairs[:, 1]]) ** 2
+            pairs = pairs[hit]
+        if not len(pairs):
+            return pos
+        redo = np.unique(np.max(pairs, axis=1))
+        pos[redo] = rng.uniform(-L / 2, L / 2, size=(len(redo), 3))
+    raise RuntimeError("bead placement did not converge (box too dense)")
 
 
 def place_beads(rng, radii, L):
@@ -141,8 +185,22 @@ class Server:
         self.memory_budget = int(memory_budget)
         self.max_active = max_active
         self.keep_positions = keep_positions
+        # device memory in use (total - free), sampled during the run
+        self.device_memory = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                def used():
+                    free, total = torch.cuda.mem_get_info()
+                    return int(total - free)
+                self.device_memory = used
+        except ImportError:
+            pass
 
-    def run(self, requests, clock="wall", tick=1e-3):
+    def run(self, requests, clock="wall", tick=1e-3, stop_admission_at=None, drain_limit=None):
+        """Serves `requests` until all are done, or -- with stop_admission_at
+        (s) -- admits nothing after that time and stops drain_limit s later
+        (then the ones still waiting or running are the backlog)."""
         reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
         for r in reqs:
             if self.batch.footprint(r.n_beads) > self.memory_budget:
@@ -153,23 +211,31 @@ class Server:
         used = 0
         peak_used, peak_active, batched_steps = 0, 0, 0
         t_step = t_admin = 0.0
+        bead_steps_done = 0
+        peak_device_used = 0
         start = time.perf_counter()
         vnow = 0.0
+        end_at = None if stop_admission_at is None else stop_admission_at + (drain_limit or 0.0)
 
         def now():
             return vnow if clock == "virtual" else time.perf_counter() - start
 
         while pending or active:
             t = now()
+            if end_at is not None and t >= end_at:
+                break
+            admitting = stop_admission_at is None or t < stop_admission_at
+            if not admitting and not active:
+                break
             # admission: arrived requests, in arrival order, while they fit
-            while pending and pending[0].arrival <= t:
+            while admitting and pending and pending[0].arrival <= t:
                 r = pending[0]
                 fp = self.batch.footprint(r.n_beads)
                 if used + fp > self.memory_budget or (self.max_active and len(active) >= self.max_active):
                     break
                 pending.popleft()
                 t0 = time.perf_counter()
-                slot = self.batch.add(r.positions, r.radii, r.box_length, T=r.T, viscosity=r.viscosity,
+                slot = self.batch.add(r.materialize(), r.radii, r.box_length, T=r.T, viscosity=r.viscosity,
                                       seed=r.seed, noise="device")
                 t_admin += time.perf_counter() - t0
                 active[slot] = [r, r.steps, fp]
@@ -180,6 +246,8 @@ class Server:
             if not active:
                 # idle until the next arrival
                 nxt = pending[0].arrival
+                if stop_admission_at is not None and nxt >= stop_admission_at:
+                    break
                 if clock == "virtual":
                     vnow = max(vnow, nxt)
                 else:
@@ -192,6 +260,9 @@ class Server:
             self.batch.propagate(dts.pop())
             t_step += time.perf_counter() - t0
             batched_steps += 1
+            bead_steps_done += sum(a[0].n_beads for a in active.values())
+            if self.device_memory and batched_steps % 16 == 1:
+                peak_device_used = max(peak_device_used, self.device_memory())
             if clock == "virtual":
                 vnow += tick
             done = []
@@ -212,20 +283,26 @@ class Server:
                     used -= fp
                 t_admin += time.perf_counter() - t0
         elapsed = now() if clock == "virtual" else time.perf_counter() - start
+        for slot in list(active):  # stopped by the drain limit: leave the batch empty
+            self.batch.remove(slot)
         recs = [records[r.rid] for r in reqs]
-        lat = np.array([x.latency for x in recs]) if recs else np.array([0.0])
-        bead_steps = sum(x.n_beads * x.steps for x in recs)
+        completed = [x for x in recs if np.isfinite(x.completed)]
+        lat = np.array([x.latency for x in completed]) if completed else np.array([math.nan])
         summary = {
             "requests": len(recs),
+            "completed": len(completed),
+            "backlog_waiting": sum(1 for x in recs if not np.isfinite(x.admitted)),
+            "backlog_running": len(active),
             "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "bead_steps_per_s": bead_steps / elapsed if elapsed > 0 else math.inf,
+            "bead_steps_per_s": bead_steps_done / elapsed if elapsed > 0 else math.inf,
             "elapsed_s": elapsed,
             "batched_steps": batched_steps,
             "peak_active": peak_active,
             "step_s": t_step,      # wall time inside batched steps (membership rebuilds included)
-            "admin_s": t_admin,    # wall time adding and removing replicas
+            "admin_s": t_admin,    # wall time adding and removing replicas (bead placement included)
             "peak_bytes": peak_used,
+            "peak_device_used_bytes": peak_device_used or None,
             "memory_budget": self.memory_budget,
         }
         return recs, summary

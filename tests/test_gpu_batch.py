@@ -327,3 +327,48 @@ def test_device_step_loop_attempt_limit():
     assert batch.last_move_attempts(other) >= 1
     assert np.allclose(batch.positions(s), pos, rtol=0, atol=1e-12)
     batch.close()
+
+
+def test_long_graph_replay_with_autotuner_matches_direct_launches():
+    """The batched configuration's shape -- 256 replicas, N uniform in
+    [32, 512] (seed 1), radii U[10, 30], volume fraction 0.05, mixed
+    precision, device noise -- stepped 200 times as graph replays (whole steps
+    on the device), then autotuned, then 200 more, against the same batch
+    stepped with every kernel launched directly (a schedule switch before
+    every step forces a rebuild, and the attempts are driven from the host):
+    identical positions bit for bit, and no step reports a failed
+    factorisation."""
+    from pybrown_b200.batch import ReplicaBatch
+    from pybrown_b200.serve import place_beads
+    rng = np.random.default_rng(1)
+    Ns = rng.integers(32, 513, size=256)
+    configs = []
+    for N in Ns:
+        radii = rng.uniform(10.0, 30.0, size=int(N))
+        L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
+        configs.append((place_beads(rng, radii, L), radii, L))
+
+    def run(direct):
+        batch = ReplicaBatch(precision="mixed")
+        slots = [batch.add(p, r, l, seed=k, noise="device") for k, (p, r, l) in enumerate(configs)]
+        snaps = []
+        for phase in range(2):
+            for step in range(200):
+                if direct:
+                    batch.set_schedule(("larger_first", "added")[step % 2])
+                batch.propagate(0.5, device_loop=not direct)
+                if not direct and step >= 1:
+                    assert batch.graph_state() == 1
+                if step % 50 == 49:
+                    snaps.append(np.concatenate([batch.positions(s).ravel() for s in slots[::17]]))
+            if phase == 0:
+                batch.autotune(reps=1)
+        final = np.concatenate([batch.positions(s).ravel() for s in slots])
+        batch.close()
+        return snaps, final
+
+    g_snaps, g_final = run(False)
+    d_snaps, d_final = run(True)
+    for a, b in zip(g_snaps, d_snaps):
+        assert np.array_equal(a, b)
+    assert np.array_equal(g_final, d_final)

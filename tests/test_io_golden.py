@@ -62,3 +62,48 @@ def test_input_data_defaults(golden, tmp_path):
     cfg.write_text(json.dumps(golden["config"]))
     inp = io.InputData(str(cfg), golden["required"], golden["defaults"], golden["all_keywords"])
     assert inp.input_data == golden["input_data"]
+
+
+def test_async_xyz_writer_bytes(golden, tmp_path):
+    """The writer thread gives the reference's bytes: frames handed over as
+    position copies (the caller goes on changing its array) and frames whose
+    buffer is filled later, behind a ready() wait."""
+    import threading
+
+    import numpy as np
+    beads = _beads(golden, tmp_path)
+    labels = [b.label for b in beads]
+    pos = np.array([b.r for b in beads])
+    xyz = tmp_path / "a.xyz"
+    with open(xyz, "w") as f, io.AsyncXYZWriter(f, "t.xyz", labels, depth=1) as w:
+        w.write(0, 0.5, pos)
+        pos[0, 0] += 0.125  # after the hand-over: frame 0 keeps the old value
+        w.write(1, 0.5, pos)
+    assert xyz.read_text() == golden["xyz_text"]
+    # a frame filled after its hand-over (an asynchronous copy in the drivers)
+    buf = np.zeros_like(pos)
+    gate = threading.Event()
+    xyz2 = tmp_path / "b.xyz"
+    with open(xyz2, "w") as f, io.AsyncXYZWriter(f, "t.xyz", labels) as w:
+        w.write(0, 0.5, np.array([b.r for b in beads]))
+        w.write(1, 0.5, buf, gate.wait)
+        buf[...] = pos
+        gate.set()
+        w.flush()
+        assert xyz2.read_text() == golden["xyz_text"]
+
+
+def test_async_xyz_writer_reraises():
+    class Broken:
+        def write(self, text):
+            raise OSError("disk full")
+
+        def flush(self):
+            pass
+
+    import numpy as np
+    w = io.AsyncXYZWriter(Broken(), "x.xyz", ["A"])
+    w.write(0, 1.0, np.zeros((1, 3)))
+    with pytest.raises(OSError):
+        w.flush()
+    w.close()

@@ -114,3 +114,42 @@ def test_placement_has_no_overlaps():
     np.fill_diagonal(dist, math.inf)
     assert np.all(dist > radii[:, None] + radii[None, :])
     assert np.all(np.abs(pos) <= L / 2)
+
+
+def test_fast_placement_has_no_overlaps_and_is_seeded():
+    from pybrown_b200.serve import place_beads_fast
+    radii = np.random.default_rng(1).uniform(10, 40, size=2048)
+    L = (np.sum(4 / 3 * np.pi * radii ** 3) / 0.05) ** (1 / 3)
+    pos = place_beads_fast(np.random.default_rng(2), radii, L)
+    assert np.array_equal(pos, place_beads_fast(np.random.default_rng(2), radii, L))
+    from scipy.spatial import cKDTree
+    pairs = cKDTree(np.mod(pos + L / 2, L), boxsize=L).query_pairs(80.0, output_type="ndarray")
+    d = pos[pairs[:, 0]] - pos[pairs[:, 1]]
+    d -= L * np.round(d / L)
+    assert np.all(np.sqrt((d ** 2).sum(1)) > radii[pairs[:, 0]] + radii[pairs[:, 1]])
+    assert np.all(np.abs(pos) <= L / 2)
+
+
+def test_lazy_stream_places_beads_on_first_use():
+    a = make_stream(5, rate=50, duration=0.4, lazy=True)
+    b = make_stream(5, rate=50, duration=0.4, lazy=True)
+    assert all(r.positions is None for r in a)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.materialize(), y.materialize())
+        assert x.materialize().shape == (x.n_beads, 3)
+
+
+def test_admission_window_and_drain_limit():
+    """Admissions stop at stop_admission_at, the loop drain_limit later: the
+    requests left are counted as backlog, latencies only over completed ones."""
+    b = FakeBatch()
+    # on the virtual clock a batched step is 1 ms; 1 runs from t=0 for 100 ms,
+    # 2 arrives after the window, 3 waits behind the concurrency cap
+    reqs = [_req(0, 0.0, 4, 5), _req(1, 0.0, 4, 100), _req(2, 0.05, 4, 5), _req(3, 0.001, 4, 3)]
+    recs, summary = Server(b, memory_budget=10 ** 9, max_active=2).run(
+        reqs, clock="virtual", tick=1e-3, stop_admission_at=0.02, drain_limit=0.03)
+    assert summary["completed"] == 2  # 0 and 3
+    assert summary["backlog_waiting"] == 1 and summary["backlog_running"] == 1
+    assert not b.slots  # everything left the batch
+    assert summary["p99_ms"] >= summary["p50_ms"] > 0
+    assert summary["elapsed_s"] == pytest.approx(0.05, abs=2e-3)
