@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "propagate.cuh"
 #include "pybrown_b200.h"
 
 namespace pbg {
@@ -154,12 +155,6 @@ namespace pbg {
 
 namespace {
 
-__device__ __forceinline__ double warp_sum(double s) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
 // B = lower(D) with the identity beyond n and zeros above the diagonal.
 template <typename T>
 __global__ void batch_copy_lower_kernel(const BatchDev* __restrict__ reps) {
@@ -186,12 +181,10 @@ __global__ void batch_det_kernel(const BatchDev* __restrict__ reps, double dt) {
   if (!r.has_force) return;
   const T* D = static_cast<const T*>(r.D);
   const double c = dt / r.kBT;
+  const double* F = r.force;
   const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
   for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < r.n; row += gridDim.x * warps) {
-    const T* a = D + (size_t)row * r.ld;
-    double s = 0.0;
-    for (int j = lane; j < r.n; j += 32) s += (c * (double)a[j]) * r.force[j];
-    s = warp_sum(s);
+    const double s = row_dot(D + (size_t)row * r.ld, r.n, [&](int j, double a) { return (c * a) * F[j]; });
     // the displacement waits in U until every row is done (see batch_det_move)
     if (lane == 0) r.U[row] = (s * 1.0) * 1.0;
   }
@@ -209,12 +202,10 @@ __global__ void batch_trmv_kernel(const BatchDev* __restrict__ reps, const unsig
   if (!mask[blockIdx.y]) return;
   const BatchDev& r = reps[blockIdx.y];
   const T* B = static_cast<const T*>(r.B);
+  const double* xi = r.xi;
   const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
   for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < r.n; row += gridDim.x * warps) {
-    const T* b = B + (size_t)row * r.ld;
-    double s = 0.0;
-    for (int j = lane; j <= row; j += 32) s += (double)b[j] * r.xi[j];
-    s = warp_sum(s);
+    const double s = row_dot(B + (size_t)row * r.ld, row + 1, [&](int j, double b) { return b * xi[j]; });
     if (lane == 0) r.U[row] = s;
   }
 }

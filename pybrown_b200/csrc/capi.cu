@@ -388,11 +388,23 @@ int pbg_get_force(pbg_system* sys, double* force_host, void* stream) {
 int pbg_set_force(pbg_system* sys, const double* force, void* stream) {
   if (!sys) return PBG_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
+  bool zero = true;
   if (!force) {
     PBG_CUDA_TRY(cudaMemsetAsync(sys->force, 0, sys->ld * sizeof(double), st));
   } else {
     PBG_CUDA_TRY(cudaMemcpyAsync(sys->force, force, sys->n * sizeof(double), cudaMemcpyDefault, st));
+    // a force in host memory is checked here: an all-zero one lets the step
+    // skip D F, whose result would be zero bit for bit
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, force) == cudaSuccess &&
+        (at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeUnregistered)) {
+      for (int i = 0; i < sys->n && zero; ++i) zero = force[i] == 0.0;
+    } else {
+      cudaGetLastError();
+      zero = false;
+    }
   }
+  sys->force_zero = zero;
   return PBG_OK;
 }
 

@@ -842,10 +842,14 @@ __device__ __forceinline__ void acc_to_smem(const T acc[16], T* s) {
 
 // Named barriers (0 is __syncthreads): arrive does not wait; both order the
 // calling threads' earlier shared-memory accesses before the barrier completes.
+// Whole warps call them; __syncwarp first reconverges a warp after divergent
+// code (the barrier instructions are warp-aligned).
 __device__ __forceinline__ void bar_arrive(int id, int count) {
+  __syncwarp();
   asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 __device__ __forceinline__ void bar_wait(int id, int count) {
+  __syncwarp();
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 

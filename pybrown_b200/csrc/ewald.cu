@@ -39,6 +39,7 @@ struct RpyArgs {
   const double* recip;  // [n_recip][8]
   const float* recip_f;
   void* M;
+  void* M_lower;        // or null: also receives the lower block triangle (tiles I >= J)
   double L, scale, alpha;
   double self_O[6], self_Q[6];
   int n, ld, smith, n_real, n_recip;
@@ -272,9 +273,14 @@ __device__ __forceinline__ void rpy_tile_body(const RpyArgs& a, int I, int J) {
   T* M = reinterpret_cast<T*>(a.M);
   const int n3 = 3 * n;
   const int row0 = 3 * I * TB, col0 = 3 * J * TB;
+  T* ML = reinterpret_cast<T*>(a.M_lower);
   for (int t = tid; t < TV * TV; t += THREADS) {
     const int r = t / TV, c = t % TV;
-    if (row0 + r < n3 && col0 + c < n3) M[(size_t)(row0 + r) * a.ld + col0 + c] = s_out[r * (TV + 1) + c];
+    if (row0 + r < n3 && col0 + c < n3) {
+      const T v = s_out[r * (TV + 1) + c];
+      M[(size_t)(row0 + r) * a.ld + col0 + c] = v;
+      if (ML) ML[(size_t)(row0 + r) * a.ld + col0 + c] = v;
+    }
   }
   if (I != J) {
     for (int t = tid; t < TV * TV; t += THREADS) {
@@ -510,7 +516,7 @@ static size_t rpy_smem_bytes(const EwaldTables* t, int precision, bool smith) {
 
 int launch_rpy_tensor(const PairSource& src, const double* pos, const double* radii, bool smith,
                       const EwaldTables* t, double scale, int precision, void* M, int ld,
-                      void* phase, cudaStream_t st) {
+                      void* phase, cudaStream_t st, void* M_lower) {
   const int n = src.n;
   const double L = src.L;
   if (n <= 0) return PBG_OK;
@@ -519,6 +525,7 @@ int launch_rpy_tensor(const PairSource& src, const double* pos, const double* ra
   a.src = src;
   a.radii = radii;
   a.M = M;
+  a.M_lower = M_lower;
   a.L = L;
   a.scale = scale;
   a.n = n;
@@ -575,6 +582,7 @@ void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool
   a.src.L = L;
   a.radii = radii;
   a.M = M;
+  a.M_lower = nullptr;
   a.L = L;
   a.scale = scale;
   a.n = n;

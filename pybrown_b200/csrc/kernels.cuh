@@ -105,9 +105,12 @@ void build_lattice_tables(double alpha, int m_max, int n_max, std::vector<double
 size_t phase_scratch_bytes(int n, const EwaldTables* t, int precision);
 // `pos` feeds the reciprocal phases (for pair-vector input pass the
 // reconstructed coordinates of launch_positions_from_pairs).
+// M_lower (optional): a second matrix that receives the same values in the
+// bead tiles on and below the block diagonal (every element of the lower
+// triangle; the rest of it is left as it was).
 int launch_rpy_tensor(const PairSource& src, const double* pos, const double* radii, bool smith,
                       const EwaldTables* t, double scale, int precision, void* M, int ld,
-                      void* phase, cudaStream_t st);
+                      void* phase, cudaStream_t st, void* M_lower = nullptr);
 
 // ---- lubrication.cu -------------------------------------------------------
 int launch_lubrication_add(const PairSource& src, const double* radii, double cutoff,

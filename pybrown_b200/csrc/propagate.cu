@@ -2,10 +2,10 @@
 // deterministic step (dt/kBT) D F, stochastic step sqrt(2 dt) B xi, the
 // midpoint drift terms, translation and the keep-in-box wrap.
 //
-// Matrix-vector products are HBM-bound: one warp per row, lanes stride over
-// the row with coalesced loads, FP64 accumulation, fixed shuffle tree (so a
-// result does not depend on scheduling).  B is lower triangular and only its
-// lower part is read.
+// Matrix-vector products are HBM-bound: one warp per row, 16-byte loads with
+// four in flight per lane (row_dot), FP64 accumulation, fixed shuffle tree
+// (so a result does not depend on scheduling).  B is lower triangular and
+// only its lower part is read.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "propagate.cuh"
@@ -14,23 +14,13 @@ namespace pbg {
 
 namespace {
 
-template <typename T>
-__device__ __forceinline__ double warp_sum(double s) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
 // y_i = sum_j fl(c * A_ij) x_j  (box.py:356: dt / kBT * D @ F).
 template <typename T>
 __global__ void gemv_scaled_kernel(const T* __restrict__ A, int ld, int n, const double* __restrict__ x,
                                    double c, double* __restrict__ y) {
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (row >= n) return;
-  const T* a = A + (size_t)row * ld;
-  double s = 0.0;
-  for (int j = lane; j < n; j += 32) s += (c * (double)a[j]) * x[j];
-  s = warp_sum<T>(s);
+  const double s = row_dot(A + (size_t)row * ld, n, [&](int j, double a) { return (c * a) * x[j]; });
   if (lane == 0) y[row] = s;
 }
 
@@ -40,11 +30,9 @@ __global__ void gemv_diff_kernel(const T* __restrict__ A, const T* __restrict__ 
                                  const double* __restrict__ x, double c, double* __restrict__ y) {
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (row >= n) return;
-  const T* a = A + (size_t)row * ld;
   const T* a0 = A0 + (size_t)row * ld;
-  double s = 0.0;
-  for (int j = lane; j < n; j += 32) s += (c * ((double)a[j] - (double)a0[j])) * x[j];
-  s = warp_sum<T>(s);
+  const double s = row_dot(A + (size_t)row * ld, n,
+                           [&](int j, double a) { return (c * (a - (double)a0[j])) * x[j]; });
   if (lane == 0) y[row] = s;
 }
 
@@ -54,10 +42,7 @@ __global__ void trmv_lower_kernel(const T* __restrict__ B, int ld, int n, const 
                                   double* __restrict__ y) {
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (row >= n) return;
-  const T* b = B + (size_t)row * ld;
-  double s = 0.0;
-  for (int j = lane; j <= row; j += 32) s += (double)b[j] * x[j];
-  s = warp_sum<T>(s);
+  const double s = row_dot(B + (size_t)row * ld, row + 1, [&](int j, double b) { return b * x[j]; });
   if (lane == 0) y[row] = s;
 }
 

@@ -289,17 +289,27 @@ static PairSource pair_source(const pbg_system* s) {
   return src;
 }
 
-// box.py:486-528.
-int compute_Dff(pbg_system* s, cudaStream_t st) {
+// box.py:486-528.  fill_B: the step factors this D next (decompose), so the
+// build also writes D's lower triangle into B.
+int compute_Dff(pbg_system* s, cudaStream_t st, bool fill_B) {
   const pbg_params& p = s->p;
   const bool smith = s->smith;
   const PairSource src = pair_source(s);
   int rc;
   if (!s->lub) {
     const double scale = p.kBT * 1e19 / p.viscosity;
-    rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, s->prec, s->D, s->ld, s->phase, st);
+    // when this step factors D, the build also writes D's lower triangle into
+    // B (the factorisation's input), so decompose needs no copy
+    void* lower = fill_B ? s->B : nullptr;
+    rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, s->prec, s->D, s->ld, s->phase, st,
+                           lower);
     if (rc) return rc;
-    return launch_pad_identity(s->D, s->n, s->ld, s->prec, st);
+    if ((rc = launch_pad_identity(s->D, s->n, s->ld, s->prec, st))) return rc;
+    if (lower) {
+      if ((rc = launch_pad_identity(s->B, s->n, s->ld, s->prec, st))) return rc;
+      s->b_holds_lower_D = true;
+    }
+    return PBG_OK;
   }
   const double scale = 1e19 / p.viscosity;
   if (s->mlub) {
@@ -379,12 +389,15 @@ int decompose(pbg_system* s, cudaStream_t st) {
     }
     return PBG_OK;
   }
-  const long long total = (long long)s->ld * s->ld;
-  if (s->prec == PBG_PREC_FP64)
-    copy_lower_pad_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)s->D, (double*)s->B, s->n, s->ld);
-  else
-    copy_lower_pad_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)s->D, (float*)s->B, s->n, s->ld);
-  PBG_CHECK_LAUNCH();
+  if (!s->b_holds_lower_D) {
+    const long long total = (long long)s->ld * s->ld;
+    if (s->prec == PBG_PREC_FP64)
+      copy_lower_pad_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)s->D, (double*)s->B, s->n, s->ld);
+    else
+      copy_lower_pad_kernel<float><<<grid_for(total), 256, 0, st>>>((const float*)s->D, (float*)s->B, s->n, s->ld);
+    PBG_CHECK_LAUNCH();
+  }
+  s->b_holds_lower_D = false;  // the factorisation overwrites it
   return launch_cholesky_ws(s->B, s->n, s->ld, s->prec, s->dflags + 1, s->chol_work, st);
 }
 
@@ -426,6 +439,8 @@ static int deterministic_step(pbg_system* s, const void* D, double mult, cudaStr
     if ((rc = launch_scale2(s->sol, s->dt, mult, s->n, s->FX, st))) return rc;
     return launch_translate(s->pos, s->FX, s->n, false, st);
   }
+  // F = 0: every term of ((dt/kBT) D F) mult is +-0 and pos + (+-0) = pos
+  if (!s->ff && s->force_zero) return PBG_OK;
   int rc = launch_gemv_scaled(D, s->ld, s->n, s->prec, step_force(s), s->dt / s->p.kBT, s->FX, st);
   if (rc) return rc;
   rc = launch_scale2(s->FX, 1.0, mult, s->n, s->FX, st);
@@ -509,7 +524,7 @@ static int divergence_step(pbg_system* s, cudaStream_t st) {
   for (int m = 0; m < n; ++m) {
     add_scalar_kernel<<<1, 32, 0, st>>>(s->pos, m, eps);
     PBG_CHECK_LAUNCH();
-    if (s->build_Dff && (rc = compute_Dff(s, st))) return rc;
+    if (s->build_Dff && (rc = compute_Dff(s, st, false))) return rc;
     if (s->build_Dnf && (rc = compute_Dtot(s, st))) return rc;
     add_row_kernel<<<(n + 255) / 256, 256, 0, st>>>((const double*)s->D, m, n, ld, s->div);
     PBG_CHECK_LAUNCH();
@@ -537,7 +552,7 @@ int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol,
   s->attempts = 0;
   int rc;
   if (s->p.hydrodynamics != PBG_HI_NONE) {
-    if (build_Dff && (rc = compute_Dff(s, st))) return rc;
+    if (build_Dff && (rc = compute_Dff(s, st, chol && !s->lub))) return rc;
     if (s->lub && build_Dnf && (rc = compute_Dtot(s, st))) return rc;
     if (chol && (rc = decompose(s, st))) return rc;
   }
@@ -570,7 +585,7 @@ static int midpoint_rebuild(pbg_system* s, cudaStream_t st) {
     return PBG_OK;
   }
   if (s->build_Dff) {
-    if ((rc = compute_Dff(s, st))) return rc;
+    if ((rc = compute_Dff(s, st, false))) return rc;
   } else {
     PBG_CUDA_TRY(cudaMemcpyAsync(s->D, s->D0, bytes, cudaMemcpyDeviceToDevice, st));
     if (s->lub) {

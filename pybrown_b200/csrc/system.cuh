@@ -29,6 +29,8 @@ struct pbg_system {
   double* radii = nullptr;     // N
   int* conn = nullptr;         // N x N bond matrix or null
   double* force = nullptr;     // ld (3N used)
+  bool force_zero = true;
+  bool b_holds_lower_D = false;  // this step's D build also wrote B's lower triangle (and padding)      // the external force is known to be zero (pbg_set_force from host or NULL)
   void* D = nullptr;           // ld x ld, prec
   void* B = nullptr;           // ld x ld, prec, lower factor
   void* D0 = nullptr;          // midpoint: step-start D
@@ -71,7 +73,7 @@ int create_system(const pbg_params* p, pbg_system** out);
 void destroy_system(pbg_system* s);
 int system_set_state(pbg_system* s, const double* pos, const double* radii, const int* conn, cudaStream_t st);
 int build_nohi(pbg_system* s, cudaStream_t st);
-int compute_Dff(pbg_system* s, cudaStream_t st);
+int compute_Dff(pbg_system* s, cudaStream_t st, bool fill_B);
 int compute_Dtot(pbg_system* s, cudaStream_t st);
 int decompose(pbg_system* s, cudaStream_t st);
 int step_begin(pbg_system* s, double dt, int build_Dff, int build_Dnf, int chol, cudaStream_t st);
