@@ -95,8 +95,13 @@ __device__ __forceinline__ int smid() {
 }
 #define TRACE(slot, t) \
   if (threadIdx.x == 0 && (t) < 65536) g_task_trace[4 * (t) + (slot)] = (slot) == 3 ? smid() : gtimer()
+// Finer timeline of the FP32 chain: 8 stamps per panel k.
+__device__ long long g_chain_trace[8 * 1024];
+#define CTRACE(k, slot) \
+  if (threadIdx.x == 0 && (k) < 1024) g_chain_trace[8 * (k) + (slot)] = gtimer()
 #else
 #define TRACE(slot, t)
+#define CTRACE(k, slot)
 #endif
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
@@ -278,17 +283,25 @@ __device__ __forceinline__ unsigned to_tf32(float x) {
 
 template <> struct TileMMA<float> {
   // mma.m16n8k8 tf32: 1 m-tile of 16 x 4 n-tiles of 8, 4 accumulators each.
+  // The product A B^T is accumulated from zero in its own registers and
+  // subtracted from acc at the end: the tensor cores' accumulation rounds at
+  // the magnitude of the product, not of the tile it updates, and acc takes
+  // one FP32 rounding per product (accumulating into acc directly made the
+  // factor's error grow with the number of panels, to 9e-6 at order 3072).
   static __device__ __forceinline__ int idx(int rs, int cs) { return (cs >> 1) * 4 + rs * 2 + (cs & 1); }
   static __device__ __forceinline__ void sub(const float* sA, const float* sB, float acc[16]) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int m0 = 16 * (w >> 1), n0 = 32 * (w & 1), g = lane >> 2, t = lane & 3;
+    float prod[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) prod[e] = 0.0f;
 #pragma unroll 2
     for (int k0 = 0; k0 < NB; k0 += 8) {
-      // split the (negated) A fragment and the B fragments into tf32 hi + lo
+      // split the A fragment and the B fragments into tf32 hi + lo
       unsigned ah[4], al[4];
       {
-        const float v[4] = {-sA[(m0 + g) * LDA + k0 + t], -sA[(m0 + g + 8) * LDA + k0 + t],
-                            -sA[(m0 + g) * LDA + k0 + t + 4], -sA[(m0 + g + 8) * LDA + k0 + t + 4]};
+        const float v[4] = {sA[(m0 + g) * LDA + k0 + t], sA[(m0 + g + 8) * LDA + k0 + t],
+                            sA[(m0 + g) * LDA + k0 + t + 4], sA[(m0 + g + 8) * LDA + k0 + t + 4]};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           ah[q] = to_tf32(v[q]);
@@ -301,7 +314,7 @@ template <> struct TileMMA<float> {
         const float v1 = sB[(n0 + 8 * nt + g) * LDA + k0 + t + 4];
         const unsigned bh0 = to_tf32(v0), bh1 = to_tf32(v1);
         const unsigned bl0 = to_tf32(v0 - __uint_as_float(bh0)), bl1 = to_tf32(v1 - __uint_as_float(bh1));
-        float* c = acc + 4 * nt;
+        float* c = prod + 4 * nt;
 #define PBG_TF32_MMA(A0, A1, A2, A3, B0, B1)                                                        \
   asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, " \
                "{%8,%9}, {%0,%1,%2,%3};"                                                            \
@@ -313,6 +326,8 @@ template <> struct TileMMA<float> {
 #undef PBG_TF32_MMA
       }
     }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] -= prod[e];
   }
 };
 
@@ -1002,6 +1017,7 @@ __device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
     float acc[16];
     TRACE(0, a.ntasks + 2 * k);
     TRACE(3, a.ntasks + 2 * k);
+    CTRACE(k, 7);
     if (k > 0) {
       if (pf_diag) {
         cp_async_wait_all();
@@ -1022,8 +1038,11 @@ __device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
     const bool have_in = s_pf[1] != 0;
     if (have_in) stage_async(tile<float>(a, k + 1, k), a.ld, Cn, LDA);
     TRACE(1, a.ntasks + 2 * k);
+    CTRACE(k, 0);
     factor_tile_f32(a, k, T, Rinv);
+    CTRACE(k, 1);
     invert_factor<float>(T, Rinv, X, Tm);
+    CTRACE(k, 2);
     {  // L_kk (zero above the diagonal) and inv(L_kk), 16 bytes per store
       float* g = tile<float>(a, k, k);
       float* inv = reinterpret_cast<float*>(a.invdiag) + (size_t)k * NB * NB;
@@ -1040,6 +1059,7 @@ __device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
       }
     }
     publish(a.fin + k * nt + k, 2);
+    CTRACE(k, 3);
     TRACE(2, a.ntasks + 2 * k);
     if (k + 1 == nt) return;
     TRACE(0, a.ntasks + 2 * k + 1);
@@ -1054,11 +1074,14 @@ __device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
     pf_diag = s_pf[0] != 0;
     if (pf_diag) stage_async(tile<float>(a, k + 1, k + 1), a.ld, sA, LDA);
     TRACE(1, a.ntasks + 2 * k + 1);
+    CTRACE(k, 4);
     solve_by_inverse(Cn, X, acc);
+    CTRACE(k, 5);
     acc_to_smem(acc, Lp);
     __syncthreads();
     store_tile(Lp, LDA, tile<float>(a, k + 1, k), a.ld);
     publish(a.fin + (k + 1) * nt + k, 1);
+    CTRACE(k, 6);
     TRACE(2, a.ntasks + 2 * k + 1);
   }
 }
@@ -1681,6 +1704,10 @@ extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(l
 #ifdef PBG_TASK_TRACE
 extern "C" __attribute__((visibility("default"))) int pbg_task_trace(long long* host, int ntasks) {
   PBG_CUDA_TRY(cudaMemcpyFromSymbol(host, g_task_trace, sizeof(long long) * 4 * ntasks));
+  return PBG_OK;
+}
+extern "C" __attribute__((visibility("default"))) int pbg_chain_trace(long long* host, int nt) {
+  PBG_CUDA_TRY(cudaMemcpyFromSymbol(host, g_chain_trace, sizeof(long long) * 8 * nt));
   return PBG_OK;
 }
 #endif

@@ -89,10 +89,12 @@ def write_to_xyz_file(xyz_file, xyz_filename, j, dt, beads):
 
 
 def _xyz_frame(xyz_filename, j, dt, labels, positions):
-    """The text of one frame in the format of write_to_xyz_file."""
-    lines = ["{}\n".format(len(labels)), "{} time [ps] {}\n".format(xyz_filename, j * dt)]
-    lines.extend("{} {} {} {}\n".format(label, *r) for label, r in zip(labels, positions))
-    return "".join(lines)
+    """The text of one frame in the format of write_to_xyz_file (the
+    shortest round-trip repr of each coordinate, as str.format gives for a
+    float), built from Python floats in one pass."""
+    x, y, z = np.asarray(positions, dtype=np.float64).reshape(-1, 3).T.tolist()
+    head = "{}\n{} time [ps] {}\n".format(len(labels), xyz_filename, j * dt)
+    return head + "".join(map("{} {!r} {!r} {!r}\n".format, labels, x, y, z))
 
 
 class AsyncXYZWriter:
