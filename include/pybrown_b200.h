@@ -374,6 +374,12 @@ PBG_API int pbg_batch_step(pbg_batch *b, double dt, int build_D, int cholesky, i
                            void *stream);
 /* D or B (PBG_MAT_D / PBG_MAT_B) of one replica, 3N x 3N FP64 row-major host array. */
 PBG_API int pbg_batch_get_matrix(pbg_batch *b, int slot, int which, double *out);
+/* Factors a copy of one replica's current D with the single-matrix
+ * factorisation (the batch's precision); *info as status[] of
+ * pbg_batch_step_end.  After a step that reported a failed factorisation it
+ * tells a matrix that is not positive definite (info > 0 again) from one the
+ * batched factorisation failed on (info 0).  The batch is left unchanged. */
+PBG_API int pbg_batch_check_factor(pbg_batch *b, int slot, int *info, void *stream);
 
 /* Schedule of the batched factorisation (no counterpart in the reference).
  * merge_order: how the replicas' task segments are interleaved in the one

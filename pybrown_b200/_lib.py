@@ -151,6 +151,7 @@ _SIGNATURES = {
     "pbg_batch_step_end": (_i, [_vp, _vp, _vp]),
     "pbg_batch_step": (_i, [_vp, _d, _i, _i, _vp, _vp, _vp]),
     "pbg_batch_get_matrix": (_i, [_vp, _i, _i, _vp]),
+    "pbg_batch_check_factor": (_i, [_vp, _i, _ip, _vp]),
     "pbg_batch_set_schedule": (_i, [_vp, _i, _i]),
     "pbg_batch_autotune": (_i, [_vp, _i, _ip, ctypes.POINTER(ctypes.c_float), _vp]),
     "pbg_batch_graph_state": (_i, [_vp]),

@@ -31,6 +31,19 @@ from . import _lib
 BOLTZMANN = 1.380649e-23  # scipy.constants.Boltzmann (box.py:636)
 
 
+class FactorisationError(_lib.PbgError):
+    """A step's factorisation failed for some replicas (the step has run for
+    all of them, so the failed replicas' moves are not to be trusted).
+    slots: {slot: status of the batched factorisation}; recheck: {slot: status
+    of a single-matrix factorisation of a copy of the same D} -- a recheck of
+    0 means the matrix was positive definite after all."""
+
+    def __init__(self, fn, code, message, slots, recheck):
+        super().__init__(fn, code, message)
+        self.slots = slots
+        self.recheck = recheck
+
+
 class ReplicaBatch:
     def __init__(self, precision="mixed", hydrodynamics="rpy_smith", ewald_alpha=None, ewald_real=2,
                  ewald_imag=4, stream=None):
@@ -128,6 +141,11 @@ class ReplicaBatch:
     def last_move_attempts(self, slot):
         return self._rep[slot]["last_move_attempts"]
 
+    def last_status(self, slot):
+        """Factorisation status of the replica in the last step: 0, the first
+        non-positive pivot (1-based), or -1 (a wait of the factorisation gave up)."""
+        return self._rep[slot].get("last_status", 0)
+
     # ---------------------------------------------------------------- schedule
     MERGE_ORDERS = ("larger_first", "added", "smaller_first", "replica_major")
 
@@ -176,10 +194,11 @@ class ReplicaBatch:
                                          status.ctypes.data, attempts.ctypes.data, st)
             for s, rec in self._rep.items():
                 rec["last_move_attempts"] = int(attempts[s])
+                rec["last_status"] = int(status[s])
             if rc == _lib.PBG_ERR_ATTEMPTS:
                 exceeded = [s for s, rec in self._rep.items() if attempts[s] >= rec["max_move_attempts"]]
                 raise AssertionError("maximal number of move attepts exceeded (slots {})".format(exceeded))
-            _lib.check("pbg_batch_step", rc)
+            self._raise_factorisation("pbg_batch_step", rc)
             return
         _lib.call("pbg_batch_step_begin", h, float(dt), int(bool(build_D)), int(bool(cholesky)), st)
         ns = _lib.lib.pbg_batch_slots(h)
@@ -218,9 +237,23 @@ class ReplicaBatch:
             self._rep[s]["last_move_attempts"] = c
         status = np.zeros(ns, dtype=np.int32)
         rc = _lib.lib.pbg_batch_step_end(h, status.ctypes.data, st)
+        for s, rec in self._rep.items():
+            rec["last_status"] = int(status[s])
         if exceeded:
             raise AssertionError("maximal number of move attepts exceeded (slots {})".format(exceeded))
-        _lib.check("pbg_batch_step_end", rc)
+        self._raise_factorisation("pbg_batch_step_end", rc)
+
+    def _raise_factorisation(self, fn, rc):
+        if rc in (_lib.PBG_ERR_NOT_SPD, _lib.PBG_ERR_BARRIER):
+            msg = _lib.last_error()
+            bad = {s: rec["last_status"] for s, rec in self._rep.items() if rec.get("last_status", 0) != 0}
+            recheck = {}
+            for s in bad:
+                info = ctypes.c_int(0)
+                if _lib.lib.pbg_batch_check_factor(self._h, int(s), ctypes.byref(info), self._stream) == _lib.PBG_OK:
+                    recheck[s] = info.value
+            raise FactorisationError(fn, rc, msg, bad, recheck)
+        _lib.check(fn, rc)
 
     def close(self):
         if self._h:

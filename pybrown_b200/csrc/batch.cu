@@ -1360,6 +1360,42 @@ PBG_API int pbg_batch_autotune(pbg_batch* b, int reps, int* best, float* ms, voi
   return rc;
 }
 
+// Factors a copy of one replica's current D with the single-matrix kernel
+// (the batch's precision) and returns its status in *info (0, a 1-based
+// non-positive pivot, or -1): after a failed batched step, tells a matrix
+// that is not positive definite from a factorisation that failed on a good
+// one.  B and the replica's state are left as they are.
+PBG_API int pbg_batch_check_factor(pbg_batch* b, int slot, int* info, void* stream) {
+  BatchReplica* r = slot_of(b, slot);
+  if (!r || !info) return PBG_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t es = elem_size(b->precision), ld = r->ld;
+  void *A = nullptr, *work = nullptr;
+  int* dinfo = nullptr;
+  const size_t wbytes = cholesky_work_bytes(r->ld, b->precision);
+  if (cudaMallocAsync(&A, ld * ld * es, st) != cudaSuccess || cudaMallocAsync(&work, wbytes, st) != cudaSuccess ||
+      cudaMallocAsync((void**)&dinfo, sizeof(int), st) != cudaSuccess) {
+    cudaGetLastError();
+    if (A) cudaFreeAsync(A, st);
+    if (work) cudaFreeAsync(work, st);
+    pbg_set_error_message("out of device memory checking a replica's factorisation");
+    return PBG_ERR_NOMEM;
+  }
+  int rc = PBG_OK;
+  if (cudaMemcpyAsync(A, r->D, ld * ld * es, cudaMemcpyDeviceToDevice, st) != cudaSuccess) rc = PBG_ERR_CUDA;
+  if (rc == PBG_OK) rc = launch_pad_identity(A, r->n, r->ld, b->precision, st);
+  if (rc == PBG_OK) rc = launch_cholesky_ws(A, r->n, r->ld, b->precision, dinfo, work, st);
+  int h = 0;
+  if (rc == PBG_OK && (cudaMemcpyAsync(&h, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = PBG_ERR_CUDA;
+  cudaFreeAsync(A, st);
+  cudaFreeAsync(work, st);
+  cudaFreeAsync(dinfo, st);
+  *info = h;
+  return rc;
+}
+
 PBG_API int pbg_batch_get_matrix(pbg_batch* b, int slot, int which, double* out) {
   BatchReplica* r = slot_of(b, slot);
   if (!r || !out || (which != PBG_MAT_D && which != PBG_MAT_B)) return PBG_ERR_ARG;

@@ -70,6 +70,7 @@ class Record:
     admitted: float = math.nan
     completed: float = math.nan
     positions: np.ndarray = field(default=None, repr=False)
+    failed: dict = None   # set when the request's factorisation failed: {"status", "recheck"}
 
     @property
     def latency(self):
@@ -197,6 +198,18 @@ class Server:
         except ImportError:
             pass
 
+    def _propagate(self, dt):
+        """One batched step; returns the replicas whose factorisation failed
+        as (slot, status, status of a single-matrix recheck)."""
+        try:
+            self.batch.propagate(dt)
+        except Exception as e:  # noqa: BLE001 -- only a failed factorisation is handled here
+            slots = getattr(e, "slots", None)
+            if not slots:
+                raise
+            return [(s, info, getattr(e, "recheck", {}).get(s)) for s, info in slots.items()]
+        return []
+
     def run(self, requests, clock="wall", tick=1e-3, stop_admission_at=None, drain_limit=None):
         """Serves `requests` until all are done, or -- with stop_admission_at
         (s) -- admits nothing after that time and stops drain_limit s later
@@ -257,8 +270,15 @@ class Server:
             if len(dts) != 1:
                 raise ValueError("requests running together must share dt")
             t0 = time.perf_counter()
-            self.batch.propagate(dts.pop())
+            failed = self._propagate(dts.pop())
             t_step += time.perf_counter() - t0
+            for slot, info, recheck in failed:
+                # a request whose factorisation failed leaves with an error; the others go on
+                r, _, fp = active.pop(slot)
+                rec = records[r.rid]
+                rec.failed = {"status": info, "recheck": recheck}
+                self.batch.remove(slot)
+                used -= fp
             batched_steps += 1
             bead_steps_done += sum(a[0].n_beads for a in active.values())
             if self.device_memory and batched_steps % 16 == 1:
@@ -288,9 +308,12 @@ class Server:
         recs = [records[r.rid] for r in reqs]
         completed = [x for x in recs if np.isfinite(x.completed)]
         lat = np.array([x.latency for x in completed]) if completed else np.array([math.nan])
+        failures = [{"rid": x.rid, "n_beads": x.n_beads, **x.failed} for x in recs if x.failed]
         summary = {
             "requests": len(recs),
             "completed": len(completed),
+            "failed": len(failures),
+            "failures": failures[:16],
             "backlog_waiting": sum(1 for x in recs if not np.isfinite(x.admitted)),
             "backlog_running": len(active),
             "p50_ms": float(np.percentile(lat, 50) * 1e3),

@@ -372,3 +372,23 @@ def test_long_graph_replay_with_autotuner_matches_direct_launches():
     for a, b in zip(g_snaps, d_snaps):
         assert np.array_equal(a, b)
     assert np.array_equal(g_final, d_final)
+
+
+def test_check_factor_of_healthy_replicas():
+    """pbg_batch_check_factor factors a copy of a replica's D with the
+    single-matrix kernel: 0 for every replica of a healthy batch, and the
+    batch's own B is left unchanged."""
+    import ctypes
+    from pybrown_b200 import _lib
+    from pybrown_b200.batch import ReplicaBatch
+    batch = ReplicaBatch(precision="mixed")
+    slots = [batch.add(*_config(800 + k, N, 0.05, 10.0, 30.0), seed=k, noise="device")
+             for k, N in enumerate((40, 130))]
+    batch.propagate(0.5)
+    for s in slots:
+        B = batch.matrix(s, "B")
+        info = ctypes.c_int(-5)
+        _lib.call("pbg_batch_check_factor", batch._h, s, ctypes.byref(info), None)
+        assert info.value == 0
+        assert np.array_equal(batch.matrix(s, "B"), B)
+    batch.close()

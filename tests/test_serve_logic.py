@@ -153,3 +153,25 @@ def test_admission_window_and_drain_limit():
     assert not b.slots  # everything left the batch
     assert summary["p99_ms"] >= summary["p50_ms"] > 0
     assert summary["elapsed_s"] == pytest.approx(0.05, abs=2e-3)
+
+
+def test_failed_factorisation_drops_only_that_request():
+    class Fail(Exception):
+        def __init__(self, slots):
+            super().__init__("factorisation failed")
+            self.slots = slots
+            self.recheck = {s: 0 for s in slots}
+
+    class FailingBatch(FakeBatch):
+        def propagate(self, dt):
+            super().propagate(dt)
+            if len(self.log) == 3 and 1 in self.slots:
+                raise Fail({1: 7})
+
+    b = FailingBatch()
+    reqs = [_req(0, 0.0, 4, 6), _req(1, 0.0, 4, 6), _req(2, 0.0, 4, 6)]
+    recs, summary = Server(b, memory_budget=10 ** 9).run(reqs, clock="virtual", tick=1e-3)
+    assert summary["failed"] == 1 and summary["completed"] == 2
+    assert recs[1].failed == {"status": 7, "recheck": 0} and math.isnan(recs[1].completed)
+    assert b.steps[0] == 6 and b.steps[2] == 6
+    assert summary["failures"][0]["rid"] == 1
