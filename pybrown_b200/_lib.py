@@ -19,6 +19,7 @@ STATUS_NAMES = {
 PBG_ERR_NOT_SPD = -3
 PBG_ERR_ATTEMPTS = -4
 PBG_ERR_NOISE = -5
+PBG_ERR_BARRIER = -7
 
 HI = {"nohi": 0, "rpy": 1, "rpy_smith": 2, "rpy_lub": 3, "rpy_smith_lub": 4}
 PREC = {"fp64": 0, "mixed": 1}

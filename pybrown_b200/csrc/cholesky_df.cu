@@ -275,6 +275,7 @@ template <> struct TileMMA<double> {
   }
 };
 
+
 __device__ __forceinline__ unsigned to_tf32(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -453,6 +454,7 @@ struct WarpTile32 {
   static __device__ __forceinline__ void mma(const float* A, int lda, const float* B, int ldb, int K, float d[4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     float d0 = 0.0f, d1 = 0.0f;
+#pragma unroll 8
     for (int k0 = 0; k0 < K; k0 += 4) {
       const float4 a4 = *reinterpret_cast<const float4*>(A + g * lda + k0);
       const float av[4] = {a4.x, a4.y, a4.z, a4.w};
@@ -916,8 +918,11 @@ __device__ __forceinline__ void factor_tile_f32(const DFArgs& a, int k, float* T
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const float d = l[j][j];
-        if (!(d > 0.0f) && bad < 0) bad = j;
-        const float rs = rsqrtf(d);
+        // a pivot below the smallest normal float (or NaN) is reported like a
+        // non-positive one; the MUFU estimate (rel. error < 2^-22) is FP32 accurate
+        if (!(d >= 1.17549435e-38f) && bad < 0) bad = j;
+        float rs;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rs) : "f"(d));
         rinv[j] = rs;
         l[j][j] = d * rs;
 #pragma unroll
@@ -974,11 +979,28 @@ __device__ __forceinline__ void factor_tile_f32(const DFArgs& a, int k, float* T
         if (c <= r) panel_update(T, r, c, c0);
       }
       bar_arrive(2, THREADS);
-      // the rest of the trailing triangle: columns >= c0 + 16
-      const int w = NB - c0 - 16;
-      for (int e = t; e < w * w; e += nthr) {
-        const int r = c0 + 16 + e / w, c = c0 + 16 + e % w;
-        if (c <= r) panel_update(T, r, c, c0);
+      // the rest of the trailing triangle, columns >= c0 + 16 and rows >= the
+      // column: thread t takes columns c0 + 16 + (t & 15) + 16 m of the rows
+      // c0 + 16 + (t >> 4) + 14 q (no integer division); each row's panel
+      // values are loaded once
+      const int cl = t & 15;
+      for (int r = c0 + 16 + (t >> 4); r < NB; r += nthr / 16) {
+        const float4 a0 = *reinterpret_cast<const float4*>(T + r * LDA + c0);
+        const float4 a1 = *reinterpret_cast<const float4*>(T + r * LDA + c0 + 4);
+        for (int c = c0 + 16 + cl; c <= r; c += 16) {
+          const float4 b0 = *reinterpret_cast<const float4*>(T + c * LDA + c0);
+          const float4 b1 = *reinterpret_cast<const float4*>(T + c * LDA + c0 + 4);
+          float v = T[r * LDA + c];
+          v = fmaf(-a0.x, b0.x, v);
+          v = fmaf(-a0.y, b0.y, v);
+          v = fmaf(-a0.z, b0.z, v);
+          v = fmaf(-a0.w, b0.w, v);
+          v = fmaf(-a1.x, b1.x, v);
+          v = fmaf(-a1.y, b1.y, v);
+          v = fmaf(-a1.z, b1.z, v);
+          v = fmaf(-a1.w, b1.w, v);
+          T[r * LDA + c] = v;
+        }
       }
     }
   }

@@ -4,12 +4,16 @@
     python -m pybrown_b200.profile_cases smith --beads 512 --precision fp64
     python -m pybrown_b200.profile_cases batch --replicas 64 --precision mixed
     python -m pybrown_b200.profile_cases lub --beads 512 --precision fp64
+    python -m pybrown_b200.profile_cases forces --beads 1024 --precision mixed
 
 `cholesky` factors the Smith-Ewald diffusion matrix of a random bead
 configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it;
 `batch` advances a batch of replicas (N uniform in [32, 512], seed 1) by one
 step; `lub` takes one midpoint step of a lubricated box (rpy_smith_lub,
-radius 20, volume fraction 0.30, cutoff 0.5, Cichocki, m = 100, dt 0.1).
+radius 20, volume fraction 0.30, cutoff 0.5, Cichocki, m = 100, dt 0.1);
+`forces` steps a box of bonded chains (16 beads each, harmonic bonds and
+angles, Lennard-Jones 6-12, rpy_smith, Ermak, dt 0.05), so that the force
+kernels run every step.
 Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
 time of one launch.
 """
@@ -42,7 +46,7 @@ def main(argv=None):
 
     from . import _lib
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("kernel", choices=("cholesky", "smith", "batch", "lub"))
+    ap.add_argument("kernel", choices=("cholesky", "smith", "batch", "lub", "forces"))
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--beads", type=int, default=256)
     ap.add_argument("--order", type=int, default=0, help="cholesky: matrix order (default 3 x beads)")
@@ -54,6 +58,8 @@ def main(argv=None):
         return _batch(a, torch)
     if a.kernel == "lub":
         return _lub(a, torch)
+    if a.kernel == "forces":
+        return _forces(a, torch)
     chol_prec = {"fp64": 0, "mixed": 1, "mixed_fp64_diag": 2}[a.precision]
     prec = min(chol_prec, 1)  # the Ewald build: FP64 or FP32
     dtype = torch.float64 if prec == 0 else torch.float32
@@ -144,6 +150,70 @@ def _lub(a, torch):
         torch.cuda.synchronize()
         total += start.elapsed_time(end)
     print(f"lub N={N} L={L:.1f} ({a.precision}): {total / a.reps:.3f} ms per step")
+
+
+def _chains(n_beads, length=16, seed=0):
+    """Straight chains of beads (radius 2, spacing 4.2 A) along random
+    directions in a box at about 2 % volume fraction, bonded along each chain
+    (rest length 4.2, k 5) with angle terms (150 degrees, k 2)."""
+    from .bead import Bead
+    rng = np.random.default_rng(seed)
+    n_chains = max(1, n_beads // length)
+    L = (n_chains * length * 4.0 / 3.0 * math.pi * 8.0 / 0.02) ** (1.0 / 3.0)
+    beads, pts_all = [], []
+    for c in range(n_chains):
+        while True:
+            start = rng.uniform(-L / 2, L / 2, 3)
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
+            pts = [start + 4.2 * i * u for i in range(length)]
+            ok = True
+            for p in pts:
+                for q in pts_all:
+                    d = p - q
+                    d -= L * np.round(d / L)
+                    if d @ d <= 4.5 ** 2:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if ok:
+                break
+        base = len(beads) + 1
+        for i, p in enumerate(pts):
+            p = p - L * np.round(p / L)
+            beads.append(Bead(p, 2.0, label="P", hard_core_radius=1.9, epsilon_LJ=0.2, bead_id=base + i))
+        pts_all.extend(pts)
+        for i in range(length - 1):
+            beads[base - 1 + i].bonded_with.append(base + i + 1)
+            beads[base - 1 + i].bonded_how[base + i + 1] = [4.2, 5.0]
+        for i in range(length - 2):
+            beads[base - 1 + i].angled_with.append([base + i + 1, base + i + 2])
+            beads[base - 1 + i].angled_how[(base + i + 1, base + i + 2)] = [150.0, 2.0]
+    return beads, L
+
+
+def _forces(a, torch):
+    from .box import Box
+    beads, L = _chains(a.beads)
+    inp = {"box_length": L, "T": 293.15, "viscosity": 0.01005, "seed": 0, "hydrodynamics": "rpy_smith",
+           "ewald_alpha": math.sqrt(math.pi), "ewald_real": 2, "ewald_imag": 4, "propagation_scheme": "ermak",
+           "immobile_labels": [], "check_overlaps": True, "overlap_treshold": 0.0, "max_move_attempts": 1000000,
+           "external_force": [0.0, 0.0, 0.0], "energy_unit": "kcal/mol", "verbose": False, "debug": False,
+           "precision": a.precision, "lennard_jones_6": True, "lennard_jones_12": True, "lennard_jones_alpha": 4.0,
+           "custom_interactions": False}
+    box = Box(beads, inp)
+    box.propagate(0.05)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(a.reps):
+        start.record()
+        box.propagate(0.05)
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    print(f"forces N={len(beads)} L={L:.1f} ({a.precision}): {total / a.reps:.3f} ms per step, E={box.E:.4g}")
 
 
 if __name__ == "__main__":
