@@ -803,27 +803,6 @@ __device__ __forceinline__ void factor_tile(const DFArgs& a, int k, T acc[16], T
   if constexpr (INVERSE) store_inverse<T, S>(a, k, Lk, Rinv, X, fs);
 }
 
-// F(k) of the mixed path: the FP32 tile in acc (after its last update) is
-// factored and inverted in FP64 (fs64 / Lk64 / X64: double scratch, [64][LDA]
-// tiles), L_kk and inv(L_kk) are stored rounded to FP32, and Xf ([64][LDA]
-// FP32 smem) receives the rounded inverse for the TF32 solves.  The two
-// accumulator layouts map (rs, cs) to the same element.
-__device__ __forceinline__ void factor_tile_fp64(const DFArgs& a, int k, const float acc[16], double* fs64,
-                                                 double* Lk64, double* X64, float* Xf) {
-  double acc64[16];
-#pragma unroll
-  for (int rs = 0; rs < 2; ++rs)
-#pragma unroll
-    for (int cs = 0; cs < 8; ++cs)
-      acc64[TileMMA<double>::idx(rs, cs)] = (double)acc[TileMMA<float>::idx(rs, cs)];
-  factor_tile<double, float>(a, k, acc64, fs64, Lk64, X64);
-  if (Xf)
-    for (int t = threadIdx.x; t < NB * NB; t += THREADS) {
-      const int r = t >> 6, c = t & 63;
-      Xf[r * LDA + c] = (float)X64[r * LDA + c];
-    }
-}
-
 // acc = -(acc + ...) helpers for S: acc = C inv(L_kk)^T with C, X in smem.
 template <typename T>
 __device__ __forceinline__ void solve_by_inverse(const T* C, const T* X, T acc[16]) {
@@ -1007,6 +986,43 @@ __device__ __forceinline__ void factor_tile_f32(const DFArgs& a, int k, float* T
   __syncthreads();
 }
 
+// L_kk from T (zero above the diagonal) into tile (k, k) of the factor and
+// inv(L_kk) from X into invdiag, 16 bytes per store.
+__device__ __forceinline__ void store_factor_inverse(const DFArgs& a, int k, const float* T, const float* X) {
+  float* g = tile<float>(a, k, k);
+  float* inv = reinterpret_cast<float*>(a.invdiag) + (size_t)k * NB * NB;
+#pragma unroll
+  for (int q = 0; q < NB * NB / 4 / THREADS; ++q) {
+    const int e = threadIdx.x + q * THREADS, r = e >> 4, c = (e & 15) * 4;
+    float4 v = *reinterpret_cast<const float4*>(T + r * LDA + c);
+    if (c + 1 > r) v.y = 0.0f;
+    if (c + 2 > r) v.z = 0.0f;
+    if (c + 3 > r) v.w = 0.0f;
+    if (c > r) v.x = 0.0f;
+    *reinterpret_cast<float4*>(g + (size_t)r * a.ld + c) = v;
+    *reinterpret_cast<float4*>(inv + r * NB + c) = *reinterpret_cast<const float4*>(X + r * LDA + c);
+  }
+}
+
+// Shared memory of an FP32 factor task: the tile, its inverse, the inversion
+// scratch (32 x 36) and 1 / L_jj.
+constexpr size_t factor_task_f32_smem_bytes() { return sizeof(float) * (2 * NB * LDA + 32 * 36 + NB); }
+
+// F(k) as a list task of the batched mixed factorisation: the updated tile
+// (acc) factored and inverted in FP32 exactly as the FP32 chain does, L_kk
+// and inv(L_kk) stored; the caller publishes.  smem is free on entry.
+__device__ __forceinline__ void factor_task_f32(const DFArgs& a, int k, const float acc[16], unsigned char* smem) {
+  float* T = reinterpret_cast<float*>(smem);
+  float* X = T + NB * LDA;
+  float* Tm = X + NB * LDA;
+  float* Rinv = Tm + 32 * 36;
+  acc_to_smem(acc, T);
+  __syncthreads();
+  factor_tile_f32(a, k, T, Rinv);
+  invert_factor<float>(T, Rinv, X, Tm);
+  store_factor_inverse(a, k, T, X);
+}
+
 // Shared memory of the FP32 chain: five [64][LDA] float tiles (the tile
 // being factored, inv(L_kk), the solve's input, the previous solve's
 // result, the prefetched next diagonal tile), the inversion scratch
@@ -1065,21 +1081,7 @@ __device__ void run_chain_f32(const DFArgs& a, unsigned char* smem, int* s_ok) {
     CTRACE(k, 1);
     invert_factor<float>(T, Rinv, X, Tm);
     CTRACE(k, 2);
-    {  // L_kk (zero above the diagonal) and inv(L_kk), 16 bytes per store
-      float* g = tile<float>(a, k, k);
-      float* inv = reinterpret_cast<float*>(a.invdiag) + (size_t)k * NB * NB;
-#pragma unroll
-      for (int q = 0; q < NB * NB / 4 / THREADS; ++q) {
-        const int e = threadIdx.x + q * THREADS, r = e >> 4, c = (e & 15) * 4;
-        float4 v = *reinterpret_cast<const float4*>(T + r * LDA + c);
-        if (c + 1 > r) v.y = 0.0f;
-        if (c + 2 > r) v.z = 0.0f;
-        if (c + 3 > r) v.w = 0.0f;
-        if (c > r) v.x = 0.0f;
-        *reinterpret_cast<float4*>(g + (size_t)r * a.ld + c) = v;
-        *reinterpret_cast<float4*>(inv + r * NB + c) = *reinterpret_cast<const float4*>(X + r * LDA + c);
-      }
-    }
+    store_factor_inverse(a, k, T, X);
     publish(a.fin + k * nt + k, 2);
     CTRACE(k, 3);
     TRACE(2, a.ntasks + 2 * k);
@@ -1425,14 +1427,16 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
 // inverse) over the same bytes and the FP64 factor scratch after them.
 template <typename T>
 constexpr size_t batch_smem_bytes() {
-  return std::max(sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>()),
-                  5 * NB * LDA * sizeof(T));  // or a paired update's five tiles
+  // an F task's factor scratch, or a paired update's five tiles
+  if constexpr (sizeof(T) == 8) return std::max(sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>()),
+                                                5 * NB * LDA * sizeof(T));
+  else return std::max(factor_task_f32_smem_bytes(), 5 * NB * LDA * sizeof(T));
 }
 
 // Two CTAs per SM in the mixed path: a second task in flight per SM hides
 // L2 latency (measured 9.8 ms against 12.4 ms for a 256-replica step at one
-// CTA per SM), at the price of a small register spill in the FP64 factor of
-// the F tasks.  One CTA per SM in the FP64 path.
+// CTA per SM).  The mixed path's F tasks factor and invert in FP32 like the
+// single-matrix FP32 chain.  One CTA per SM in the FP64 path.
 template <typename T>
 __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
                                                                  const int4* __restrict__ tasks, int ntasks,
@@ -1503,7 +1507,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
       }
       if (type == TASK_F) {
         if constexpr (sizeof(T) == 8) factor_tile<double>(a, col, acc, fs64, Lk64, X64);
-        else factor_tile_fp64(a, col, acc, fs64, Lk64, X64, nullptr);
+        else factor_task_f32(a, col, acc, smem);
       } else {
         if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
         stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);

@@ -15,7 +15,8 @@ radius 20, volume fraction 0.30, cutoff 0.5, Cichocki, m = 100, dt 0.1);
 angles, Lennard-Jones 6-12, rpy_smith, Ermak, dt 0.05), so that the force
 kernels run every step.
 Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
-time of one launch.
+time of one launch; `--reps 0` runs the warm-up call only (a batch's first
+step is made of direct kernel launches, the later ones replay a CUDA graph).
 """
 import argparse
 import math
@@ -39,6 +40,28 @@ def _config(seed, n, L, a_lo=10.0, a_hi=40.0, gap=0.0):
         pos[k], radii[k] = p, a
         k += 1
     return pos, radii
+
+
+def _time(torch, fn, reps):
+    """Mean CUDA-event time (ms) of `reps` calls of fn after one warm-up call;
+    None for reps = 0 (the warm-up call only)."""
+    fn()
+    torch.cuda.synchronize()
+    if reps <= 0:
+        return None
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(reps):
+        start.record()
+        fn()
+        end.record()
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    return total / reps
+
+
+def _ms(t):
+    return "warm-up only" if t is None else f"{t:.3f} ms"
 
 
 def main(argv=None):
@@ -86,19 +109,9 @@ def main(argv=None):
         M.copy_(A0)
         _lib.call("pbg_dev_cholesky", M.data_ptr(), n, ld, chol_prec, info.data_ptr(), None)
 
-    fn = smith if a.kernel == "smith" else cholesky
-    fn()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    total = 0.0
-    for _ in range(a.reps):
-        start.record()
-        fn()
-        end.record()
-        torch.cuda.synchronize()
-        total += start.elapsed_time(end)
+    t = _time(torch, smith if a.kernel == "smith" else cholesky, a.reps)
     extra = f" info={int(info.item())}" if a.kernel == "cholesky" else ""
-    print(f"{a.kernel} n={n} ({a.precision}): {total / a.reps:.3f} ms per launch{extra}")
+    print(f"{a.kernel} n={n} ({a.precision}): {_ms(t)} per launch{extra}")
 
 
 def _batch(a, torch):
@@ -111,17 +124,8 @@ def _batch(a, torch):
         radii = rng.uniform(10.0, 30.0, size=int(N))
         L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
         batch.add(place_beads(rng, radii, L), radii, L, seed=k, noise="device")
-    batch.propagate(0.5)
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    total = 0.0
-    for _ in range(a.reps):
-        start.record()
-        batch.propagate(0.5)
-        end.record()
-        torch.cuda.synchronize()
-        total += start.elapsed_time(end)
-    print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}): {total / a.reps:.3f} ms per step")
+    t = _time(torch, lambda: batch.propagate(0.5), a.reps)
+    print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}): {_ms(t)} per step")
     batch.close()
 
 
@@ -139,17 +143,8 @@ def _lub(a, torch):
            "precision": a.precision, "lennard_jones_6": False, "lennard_jones_12": False,
            "custom_interactions": False}
     box = Box([Bead(p, r) for p, r in zip(pos, radii)], inp)
-    box.propagate(0.1)
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    total = 0.0
-    for _ in range(a.reps):
-        start.record()
-        box.propagate(0.1)
-        end.record()
-        torch.cuda.synchronize()
-        total += start.elapsed_time(end)
-    print(f"lub N={N} L={L:.1f} ({a.precision}): {total / a.reps:.3f} ms per step")
+    t = _time(torch, lambda: box.propagate(0.1), a.reps)
+    print(f"lub N={N} L={L:.1f} ({a.precision}): {_ms(t)} per step")
 
 
 def _chains(n_beads, length=16, seed=0):
@@ -203,17 +198,8 @@ def _forces(a, torch):
            "precision": a.precision, "lennard_jones_6": True, "lennard_jones_12": True, "lennard_jones_alpha": 4.0,
            "custom_interactions": False}
     box = Box(beads, inp)
-    box.propagate(0.05)
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    total = 0.0
-    for _ in range(a.reps):
-        start.record()
-        box.propagate(0.05)
-        end.record()
-        torch.cuda.synchronize()
-        total += start.elapsed_time(end)
-    print(f"forces N={len(beads)} L={L:.1f} ({a.precision}): {total / a.reps:.3f} ms per step, E={box.E:.4g}")
+    t = _time(torch, lambda: box.propagate(0.05), a.reps)
+    print(f"forces N={len(beads)} L={L:.1f} ({a.precision}): {_ms(t)} per step, E={box.E:.4g}")
 
 
 if __name__ == "__main__":
