@@ -385,14 +385,27 @@ PBG_API int pbg_batch_check_factor(pbg_batch *b, int slot, int *info, void *stre
  * merge_order: how the replicas' task segments are interleaved in the one
  * task list; ctas_per_sm: resident CTAs per SM of the persistent kernel
  * (0 = as many as fit).  No choice changes any result bit. */
-enum { PBG_MERGE_LARGER_FIRST = 0, PBG_MERGE_ADDED = 1, PBG_MERGE_SMALLER_FIRST = 2, PBG_MERGE_REPLICA_MAJOR = 3 };
+enum {
+  PBG_MERGE_LARGER_FIRST = 0,
+  PBG_MERGE_ADDED = 1,
+  PBG_MERGE_SMALLER_FIRST = 2,
+  PBG_MERGE_REPLICA_MAJOR = 3,
+  /* larger first, in consecutive chunks of replicas whose matrices together
+   * fit 32 / 64 / 128 MiB (the chunks' segments interleaved within a chunk,
+   * chunk after chunk), so that a tile is still in L2 for its next update */
+  PBG_MERGE_CHUNK_32M = 4,
+  PBG_MERGE_CHUNK_64M = 5,
+  PBG_MERGE_CHUNK_128M = 6
+};
+#define PBG_MERGE_ORDERS 7
 PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_sm);
 /* Autotuner: after a step has built D (not inside a step), times `reps`
- * factorisations of the current matrices under every schedule (the four
- * merge orders x 1 or 2 CTAs per SM in FP32, 1 in FP64), keeps the fastest
- * and leaves B as the factor of the current D (the value a step would give).
- * best[2] = {merge_order, ctas_per_sm}; ms (may be NULL) receives the mean
- * time of each candidate, merge order major (8 entries). */
+ * factorisations of the current matrices under every schedule (the
+ * PBG_MERGE_ORDERS merge orders x 1 or 2 CTAs per SM in FP32, 1 in FP64),
+ * keeps the fastest and leaves B as the factor of the current D (the value a
+ * step would give).  best[2] = {merge_order, ctas_per_sm}; ms (may be NULL)
+ * receives the mean time of each candidate, merge order major
+ * (2 * PBG_MERGE_ORDERS entries; -1 for a candidate not run). */
 PBG_API int pbg_batch_autotune(pbg_batch *b, int reps, int *best, float *ms, void *stream);
 /* How the start of a step (Ewald build, copy into B, factorisation,
  * deterministic move) -- or with pbg_batch_step the whole step -- runs:

@@ -147,7 +147,8 @@ class ReplicaBatch:
         return self._rep[slot].get("last_status", 0)
 
     # ---------------------------------------------------------------- schedule
-    MERGE_ORDERS = ("larger_first", "added", "smaller_first", "replica_major")
+    MERGE_ORDERS = ("larger_first", "added", "smaller_first", "replica_major",
+                    "chunk_32M", "chunk_64M", "chunk_128M")
 
     def set_schedule(self, merge_order="larger_first", ctas_per_sm=0):
         """Schedule of the batched factorisation: the interleaving of the
@@ -159,10 +160,11 @@ class ReplicaBatch:
         """Times the factorisation of the current matrices under every
         schedule (after a step, between steps), keeps the fastest and returns
         {"merge_order", "ctas_per_sm", "ms": {(merge_order, ctas): mean ms}}."""
+        n = 2 * len(self.MERGE_ORDERS)
         best = (ctypes.c_int * 2)()
-        ms = (ctypes.c_float * 8)()
+        ms = (ctypes.c_float * n)()
         _lib.call("pbg_batch_autotune", self._h, int(reps), best, ms, self._stream)
-        table = {(self.MERGE_ORDERS[k // 2], k % 2 + 1): float(ms[k]) for k in range(8) if ms[k] >= 0}
+        table = {(self.MERGE_ORDERS[k // 2], k % 2 + 1): float(ms[k]) for k in range(n) if ms[k] >= 0}
         return {"merge_order": self.MERGE_ORDERS[best[0]], "ctas_per_sm": int(best[1]), "ms": table}
 
     def graph_state(self):

@@ -173,6 +173,21 @@ __global__ void batch_copy_lower_kernel(const BatchDev* __restrict__ reps) {
   }
 }
 
+// The padding rows of B's lower triangle: identity (rows n .. ld-1, columns
+// up to the diagonal).  The rest of the lower triangle comes from the Ewald
+// build; nothing reads B above the diagonal.
+template <typename T>
+__global__ void batch_pad_lower_kernel(const BatchDev* __restrict__ reps) {
+  const BatchDev& r = reps[blockIdx.y];
+  T* dst = static_cast<T*>(r.B);
+  const int n = r.n, ld = r.ld;
+  const long long total = (long long)(ld - n) * ld;
+  for (long long t = threadIdx.x; t < total; t += blockDim.x) {
+    const int row = n + (int)(t / ld), col = (int)(t % ld);
+    if (col <= row) dst[(size_t)row * ld + col] = (T)(row == col ? 1 : 0);
+  }
+}
+
 // Deterministic step (box.py:353-362) for replicas with a force:
 // pos += ((dt/kBT) D @ F * 1) * 1, one warp per row.
 template <typename T>
@@ -551,7 +566,7 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
     d.check = r->p.check_overlaps;
     d.has_force = r->has_force;
     d.pad = 0;
-    rpy_batch_arg(r->pos, r->radii, r->N, r->p.box_length, smith, b->tables, r->scale, r->D, r->ld, r->phase,
+    rpy_batch_arg(r->pos, r->radii, r->N, r->p.box_length, smith, b->tables, r->scale, r->D, r->B, r->ld, r->phase,
                   rpy.data() + q * rpy_batch_arg_bytes());
     CholRep& c = chol[q];
     c.A = r->B;
@@ -566,8 +581,9 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
   }
   // Merge order of the replicas' task segments (see cholesky_df.cu): by
   // segment number with larger matrices first (default), in the order the
-  // replicas were added, smaller first, or replica after replica (all of
-  // one replica's segments, larger replicas first).  Each replica's own
+  // replicas were added, smaller first, replica after replica (all of one
+  // replica's segments, larger replicas first), or larger first in chunks of
+  // replicas whose matrices fit a byte budget, chunk after chunk.  Each replica's own
   // segments keep their order in every policy, so every task still depends
   // only on earlier tasks.
   std::vector<int> order(R);
@@ -592,6 +608,22 @@ int rebuild(pbg_batch* b, cudaStream_t st) {
   if (b->merge_order == PBG_MERGE_REPLICA_MAJOR) {
     for (int q : order)
       for (int sg = 0; sg < max_seg; ++sg) push_seg(q, sg);
+  } else if (b->merge_order >= PBG_MERGE_CHUNK_32M) {
+    // chunks of consecutive (larger-first) replicas within the byte budget
+    const size_t budget = (size_t)32 << (20 + (b->merge_order - PBG_MERGE_CHUNK_32M));
+    const size_t es = b->precision == PBG_PREC_FP64 ? 8 : 4;
+    for (size_t c0 = 0; c0 < order.size();) {
+      size_t c1 = c0, bytes = 0;
+      do {
+        const BatchReplica* r = b->slots[b->active[order[c1]]];
+        bytes += (size_t)r->ld * r->ld * es;
+        ++c1;
+      } while (c1 < order.size() && bytes + (size_t)b->slots[b->active[order[c1]]]->ld *
+                                                b->slots[b->active[order[c1]]]->ld * es <= budget);
+      for (int sg = 0; sg < max_seg; ++sg)
+        for (size_t q = c0; q < c1; ++q) push_seg(order[q], sg);
+      c0 = c1;
+    }
   } else {
     for (int sg = 0; sg < max_seg; ++sg)
       for (int q : order) push_seg(q, sg);
@@ -896,12 +928,21 @@ static int enqueue_begin(pbg_batch* b, double dt, int build_D, int cholesky, boo
   const bool f64 = b->precision == PBG_PREC_FP64;
   const bool smith = b->hydrodynamics == PBG_HI_RPY_SMITH;
   int rc;
-  if (build_D && (rc = launch_rpy_batch(b->precision, smith, b->tables, b->d_rpy, b->d_ework, b->n_ework, R, st)))
+  // a step that builds and factors D has the Ewald build write D's lower
+  // triangle into B as well; only B's padding rows are then set here
+  if (build_D && (rc = launch_rpy_batch(b->precision, smith, b->tables, b->d_rpy, b->d_ework, b->n_ework, R,
+                                        cholesky != 0, st)))
     return rc;
   if (cholesky) {
-    const dim3 g(64, R);
-    if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
-    else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+    if (build_D) {
+      const dim3 g(1, R);
+      if (f64) batch_pad_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
+      else batch_pad_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+    } else {
+      const dim3 g(64, R);
+      if (f64) batch_copy_lower_kernel<double><<<g, 256, 0, st>>>(b->d_reps);
+      else batch_copy_lower_kernel<float><<<g, 256, 0, st>>>(b->d_reps);
+    }
     PBG_CHECK_LAUNCH();
     PBG_CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, b->flag_ints * sizeof(int), st));
     if ((rc = launch_cholesky_batch(b->precision, b->d_chol, b->d_tasks, b->ntasks, b->d_flags, b->ctas_per_sm, st)))
@@ -1276,7 +1317,7 @@ PBG_API int pbg_batch_step_end(pbg_batch* b, int* status, void* stream) {
 // D or B (which = PBG_MAT_D / PBG_MAT_B) of one replica as a 3N x 3N FP64
 // row-major host array.
 PBG_API int pbg_batch_set_schedule(pbg_batch* b, int merge_order, int ctas_per_sm) {
-  if (!b || merge_order < PBG_MERGE_LARGER_FIRST || merge_order > PBG_MERGE_REPLICA_MAJOR || ctas_per_sm < 0)
+  if (!b || merge_order < PBG_MERGE_LARGER_FIRST || merge_order >= PBG_MERGE_ORDERS || ctas_per_sm < 0)
     return PBG_ERR_ARG;
   if (b->in_step) {
     pbg_set_error_message("pbg_batch_set_schedule inside a step");
@@ -1302,7 +1343,7 @@ PBG_API int pbg_batch_autotune(pbg_batch* b, int reps, int* best, float* ms, voi
   const bool f64 = b->precision == PBG_PREC_FP64;
   const int max_ctas = f64 ? 1 : 2;
   if (ms)
-    for (int c = 0; c < 8; ++c) ms[c] = -1.0f;
+    for (int c = 0; c < 2 * PBG_MERGE_ORDERS; ++c) ms[c] = -1.0f;
   const int old_order = b->merge_order, old_ctas = b->ctas_per_sm;
   float best_ms = -1.0f;
   best[0] = old_order;
@@ -1311,7 +1352,7 @@ PBG_API int pbg_batch_autotune(pbg_batch* b, int reps, int* best, float* ms, voi
   PBG_CUDA_TRY(cudaEventCreate(&e0));
   PBG_CUDA_TRY(cudaEventCreate(&e1));
   int rc = PBG_OK;
-  for (int order = PBG_MERGE_LARGER_FIRST; order <= PBG_MERGE_REPLICA_MAJOR && rc == PBG_OK && R; ++order) {
+  for (int order = PBG_MERGE_LARGER_FIRST; order < PBG_MERGE_ORDERS && rc == PBG_OK && R; ++order) {
     for (int ctas = 1; ctas <= max_ctas && rc == PBG_OK; ++ctas) {
       b->merge_order = order;
       b->ctas_per_sm = ctas;

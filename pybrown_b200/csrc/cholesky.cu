@@ -56,18 +56,22 @@ int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* w
   return launch_cholesky_df(A, n, ld, precision, info, inv_tiles, df, st);
 }
 
-size_t spd_inverse_work_bytes(int ld) {
-  // inv(L_kk) tiles + X = inv(L) (ld x ld)
-  return cholesky_work_bytes(ld, PBG_PREC_FP64) + (size_t)ld * ld * sizeof(double);
-}
+// Workspace: the factorisation's (inv(L_kk) tiles, data-flow scratch), then
+// X = inv(L) (ld x ld) from the next 256-byte boundary.
+static size_t spd_x_offset(int ld) { return (cholesky_work_bytes(ld, PBG_PREC_FP64) + 255) / 256 * 256; }
 
+size_t spd_inverse_work_bytes(int ld) { return spd_x_offset(ld) + (size_t)ld * ld * sizeof(double); }
+
+// inv(A) = X^T X with X = inv(L): one data-flow launch factors A and forms
+// X's off-diagonal tiles, then X's diagonal tiles and the symmetric product.
 int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st) {
   const int nt = ld / NB;
-  double* W = (double*)work;
-  double* X = W + (size_t)nt * NB * NB;
-  int rc = launch_cholesky_ws(A, n, ld, PBG_PREC_FP64, info, W, st);
+  unsigned char* w = static_cast<unsigned char*>(work);
+  double* inv = reinterpret_cast<double*>(w);
+  double* X = reinterpret_cast<double*>(w + spd_x_offset(ld));
+  int rc = launch_cholesky_df(A, n, ld, PBG_PREC_FP64, info, inv, w + (size_t)nt * NB * NB * sizeof(double), st, X);
   if (rc != PBG_OK) return rc;
-  if ((rc = launch_trtri_tc(A, W, X, ld, PBG_PREC_FP64, st))) return rc;
+  if ((rc = launch_trtri_diag(inv, X, ld, PBG_PREC_FP64, st))) return rc;
   return launch_lauum_tc(X, ld, 1.0, false, A, PBG_PREC_FP64, st);
 }
 

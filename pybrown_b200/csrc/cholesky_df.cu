@@ -40,6 +40,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tc_tile.cuh"
 
 namespace pbg {
 
@@ -51,9 +52,13 @@ constexpr int TILE_PER_THREAD = 64 * 64 / THREADS;  // elements of a 64 x 64 til
 constexpr int LDA = NB + 4;   // staged tile row (bank-conflict-free fragment and row loads)
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
-// TASK_U2 / TASK_U3: U(i, j, k), U(i+1, j, k) (and U(i+2, j, k)) as one task
-// (they share L_jk).  Triples only in the FP32 single-matrix list.
-enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3, TASK_U2 = 4, TASK_U3 = 5 };
+// TASK_U2 / TASK_U3 / TASK_U4: U(i, j, k) .. U(i+r-1, j, k) as one task (they
+// share L_jk).  Groups of three and four rows only in the FP32 single-matrix
+// list, whose update tasks run on the tcgen05 tensor cores.
+enum : int { TASK_F = 0, TASK_S = 1, TASK_U = 2, TASK_I = 3, TASK_U2 = 4, TASK_U3 = 5, TASK_U4 = 6 };
+// XG / XZ: the tasks that form X = inv(L) in the same list (single-matrix
+// lists of an SPD inverse only; see inverse_update / inverse_finish).
+enum : int { TASK_XG = 7, TASK_XZ = 8 };
 
 struct DFArgs {
   void* A;
@@ -66,6 +71,9 @@ struct DFArgs {
   void* invdiag; // nt * 64 * 64 (T): inv(L_kk), row-major tiles
   unsigned* err;
   long long spin_limit;  // polls before a wait gives up
+  void* X;       // or null: X = inv(L) is formed too (off-diagonal tiles of the ld x ld matrix)
+  int* xupd;     // nt * nt: terms applied to X's tile (i, j)
+  int* xfin;     // nt * nt: X's tile (i, j) final
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -107,7 +115,7 @@ __device__ long long g_chain_trace[8 * 1024];
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 
-// Warp 0 waits until every flags[q] >= targets[q] (count <= 7, bounded);
+// Warp 0 waits until every flags[q] >= targets[q] (count <= 9, bounded);
 // returns false if the run was aborted.  Lane q polls flag q, so one round
 // costs one L2 round trip whatever the count.  The acquire loads followed by
 // the CTA barrier order every thread's later reads after the producers'
@@ -118,7 +126,7 @@ __device__ bool wait_all(const DFArgs& a, const int* const* flags, const int* ta
     const int* flag = nullptr;
     int target = 0;
 #pragma unroll
-    for (int q = 0; q < 7; ++q)  // compile-time indices: the arrays stay in registers
+    for (int q = 0; q < 9; ++q)  // compile-time indices: the arrays stay in registers
       if (q < count && q == lane) {
         flag = flags[q];
         target = targets[q];
@@ -1274,49 +1282,235 @@ __device__ __forceinline__ void update_tile_pair(const DFArgs& a, int i, int j, 
   store_tile(sC2, LDA, tile<T>(a, i + 1, j), a.ld);
 }
 
-// U(i, j, k), U(i+1, j, k), U(i+2, j, k) together: seven tiles in one round of
-// 16-byte copies, three accumulators against the shared L_jk.  s: seven
-// [64][LDA] T tiles.
-template <typename T>
-__device__ __forceinline__ void update_tile_triple(const DFArgs& a, int i, int j, int k, T acc[16], T* s) {
-  T* sB = s;
-  T* sA[3] = {s + NB * LDA, s + 2 * NB * LDA, s + 3 * NB * LDA};
-  T* sC[3] = {s + 4 * NB * LDA, s + 5 * NB * LDA, s + 6 * NB * LDA};
-  stage_async(tile<T>(a, j, k), a.ld, sB, LDA);
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    if (r > 0 || i != j) stage_async(tile<T>(a, i + r, k), a.ld, sA[r], LDA);
-    stage_async(tile<T>(a, i + r, j), a.ld, sC[r], LDA);
-  }
-  cp_async_wait_all();
+// ---------------------------------------------------------------- tcgen05 updates
+// The FP32 lists' update tasks run on the 5th-generation tensor cores: a task
+// U(i .. i+rows-1, j, k) (rows <= 4, sharing L_jk) splits L_jk and the rows'
+// L_ik into TF32 hi / lo halves in swizzled shared memory, one thread issues
+// P = L_ik L_jk^T as 3xTF32 MMAs (M = 128: two row tiles per MMA, N = 64,
+// K = 64) into TMEM accumulators (from zero), and the warps read P back with
+// tcgen05.ld and subtract it from C_ij (C -= P once, as the mma.sync
+// products do).  Each worker CTA allocates its 128 TMEM columns once.
+struct TcWorker {
+  uint64_t* mbar;       // MMA completion (one phase per task)
+  uint32_t tmem;        // TMEM base: one accumulator of 64 columns per row pair
+  uint32_t phase;
+  int max_pairs;        // row pairs per task: 2 (single matrix) or 1 (batch)
+  unsigned char* base;  // 1024-byte aligned operand area
+};
+constexpr uint32_t TC_A_BYTES = tc::operand_bytes(128);  // one M = 128 operand half (hi or lo)
+constexpr uint32_t TC_B_BYTES = tc::operand_bytes(64);
+// A hi, A lo (max_pairs row pairs each), B hi, B lo, and the alignment slack
+constexpr size_t tc_worker_smem_bytes(int max_pairs) { return 2 * max_pairs * TC_A_BYTES + 2 * TC_B_BYTES + 1024; }
+// TMEM columns: a power of two >= 32
+__host__ __device__ constexpr uint32_t tc_cols(int max_pairs) { return max_pairs > 1 ? 128u : 64u; }
+
+__device__ __forceinline__ void tc_worker_begin(uint64_t* mbar, uint32_t* s_tmem, unsigned char* smem, int max_pairs,
+                                                TcWorker& w) {
+  if (threadIdx.x == 0) tc::mbar_init(mbar, 1);
+  if (threadIdx.x < 32) tc::tmem_alloc(s_tmem, tc_cols(max_pairs));
+  tc::fence_before_sync();
   __syncthreads();
-  T acc2[16], acc3[16];
-  smem_to_acc(sC[0], acc);
-  smem_to_acc(sC[1], acc2);
-  smem_to_acc(sC[2], acc3);
-  TileMMA<T>::sub(i != j ? sA[0] : sB, sB, acc);
-  TileMMA<T>::sub(sA[1], sB, acc2);
-  TileMMA<T>::sub(sA[2], sB, acc3);
-  acc_to_smem(acc, sC[0]);  // each thread rewrites the elements it read
-  acc_to_smem(acc2, sC[1]);
-  acc_to_smem(acc3, sC[2]);
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 3; ++r) store_tile(sC[r], LDA, tile<T>(a, i + r, j), a.ld);
+  tc::fence_after_sync();
+  w.mbar = mbar;
+  w.tmem = *s_tmem;
+  w.phase = 0;
+  w.max_pairs = max_pairs;
+  w.base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
 }
 
-// F32CHAIN (FP32 matrices only): the chain CTA runs the FP32 chain
-// (run_chain_f32) and the task list has no I(k) tasks; otherwise run_chain,
-// whose diagonal tiles are factored in FP64.
-template <typename T, bool F32CHAIN>
-__global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_task, s_ok;
-  if (blockIdx.x == 0) {
-    if constexpr (F32CHAIN) run_chain_f32(a, smem, &s_ok);
-    else run_chain<T>(a, smem, &s_ok);
-    return;
+__device__ __forceinline__ void tc_worker_end(const TcWorker& w) {
+  tc::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x < 32) tc::tmem_dealloc(w.tmem, tc_cols(w.max_pairs));
+}
+
+// U(i + r, j, k) for r < rows (rows <= 2 max_pairs) on the tensor cores (the
+// dependencies are met).  Returns false if the MMAs did not complete within
+// the spin limit (the run is then aborted like an expired flag wait).
+__device__ bool update_rows_tc(const DFArgs& a, int i, int rows, int j, int k, TcWorker& w) {
+  unsigned char* Ahi = w.base;
+  unsigned char* Alo = Ahi + w.max_pairs * TC_A_BYTES;
+  unsigned char* Bhi = Alo + w.max_pairs * TC_A_BYTES;
+  unsigned char* Blo = Bhi + TC_B_BYTES;
+  const int pairs = (rows + 1) >> 1;
+  {
+    // L_jk and the rows' L_ik, all loads in flight together
+    tc::SplitTile t[5];
+    t[0] = tc::SplitTile{tile<float>(a, j, k), 64, 0, Bhi, Blo};
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      t[1 + r] = tc::SplitTile{tile<float>(a, i + (r < rows ? r : 0), k), 128, 64 * (r & 1),
+                               Ahi + (r >> 1) * TC_A_BYTES, Alo + (r >> 1) * TC_A_BYTES};
+    tc::split_tiles_all<THREADS, 5>(t, 1 + rows, a.ld);
   }
+  tc::fence_proxy_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::fence_after_sync();
+    for (int p = 0; p < pairs; ++p)
+      tc::issue_product(w.tmem + 64 * p, tc::smem_u32(Ahi + p * TC_A_BYTES), tc::smem_u32(Alo + p * TC_A_BYTES),
+                        tc::smem_u32(Bhi), tc::smem_u32(Blo));
+    tc::mma_commit(w.mbar);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = warp & 3, g = warp >> 2;
+  const int m = 32 * q + lane;  // accumulator row = TMEM lane
+  const int p = pairs == 2 ? g : 0;
+  const int c0 = pairs == 2 ? 0 : 32 * g;
+  const int nh = pairs == 2 ? 2 : 1;  // 32-column halves this warp reads
+  const int rr = 2 * p + (m >> 6);    // row tile in the group (warp-uniform)
+  bool ok = tc::mbar_wait(w.mbar, w.phase, a.spin_limit);
+  if (!ok) tc::mbar_wait(w.mbar, w.phase, a.spin_limit);  // the MMAs must not outlive the TMEM
+  ok = __syncthreads_and(ok) != 0;                          // one verdict for the whole CTA
+  if (!ok && threadIdx.x == 0) {
+    atomicExch(a.ctl + 1, 1);
+    atomicOr(a.err, PBG_DEV_ERR_BARRIER);
+    atomicCAS(a.info, 0, -1);
+  }
+  w.phase ^= 1;
+  tc::fence_after_sync();
+  // P from TMEM into shared memory, row-major [rows * 64][LDA] over the A
+  // operands (the MMAs that read them are complete) ...
+  float* Ps = reinterpret_cast<float*>(w.base);
+  if (ok && rr < rows) {
+    for (int h = 0; h < nh; ++h) {
+      float v[32];
+      tc::tmem_ld32(w.tmem + ((uint32_t)(32 * q) << 16) + 64 * p + c0 + 32 * h, v);
+      float* dst = Ps + (size_t)(64 * rr + (m & 63)) * LDA + c0 + 32 * h;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        *reinterpret_cast<float4*>(dst + 4 * u) = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+    }
+  }
+  __syncthreads();
+  // ... then C -= P with coalesced 16-byte accesses (a row of 64 per 16 threads)
+  if (ok)
+    for (int e = threadIdx.x; e < rows * NB * 16; e += THREADS) {
+      const int row = e >> 4, c4 = e & 15;
+      float4* gp = reinterpret_cast<float4*>(tile<float>(a, i + (row >> 6), j) + (size_t)(row & 63) * a.ld) + c4;
+      float4 cv = __ldcg(gp);
+      const float4 pv = *reinterpret_cast<const float4*>(Ps + (size_t)row * LDA + 4 * c4);
+      cv.x -= pv.x;
+      cv.y -= pv.y;
+      cv.z -= pv.z;
+      cv.w -= pv.w;
+      *gp = cv;
+    }
+  tc::fence_before_sync();
+  __syncthreads();
+  return ok;
+}
+
+// ---------------------------------------------------------------- inv(L) in the task list
+// With DFArgs::X set, the factorisation's task list also forms X = inv(L)
+// (its off-diagonal tiles; the diagonal ones are the inv(L_kk) in invdiag),
+// right-looking over the columns of L:
+//   X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj    (i > j),
+// accumulated as V_ij = -sum_k L_ik X_kj in X's own tile (i, j), in k order:
+//   XG(i, j, k), j <= k <= i-2: V_ij -= L_ik X_kj for rows i and i+1 (they
+//     share X_kj); needs L_ik final, X_kj final and the k - j earlier terms;
+//   XZ(i, j): V_ij -= L_{i,i-1} X_{i-1,j}, then X_ij = X_ii V_ij; needs
+//     L_{i,i-1}, X_{i-1,j}, inv(L_ii) (fin(i,i) = 2) and the earlier terms.
+// xupd(i, j) counts the applied terms, xfin(i, j) = 1 marks X_ij final.  The
+// list places XZ(k+1, .) and XG(., ., k) right after panel k's block, after
+// every task (or chain step) they depend on.  Tiles written in this kernel
+// are read through L2 (.cg loads, cp.async.cg).
+
+template <typename T>
+__device__ __forceinline__ const T* xtile(const DFArgs& a, int k, int j) {
+  return k == j ? reinterpret_cast<const T*>(a.invdiag) + (size_t)j * NB * NB
+                : reinterpret_cast<const T*>(a.X) + (size_t)k * NB * a.ld + (size_t)j * NB;
+}
+template <typename T>
+__device__ __forceinline__ T* xtile_out(const DFArgs& a, int i, int j) {
+  return reinterpret_cast<T*>(a.X) + (size_t)i * NB * a.ld + (size_t)j * NB;
+}
+
+// s[c][r] = g[r][c] through L2, all of a thread's loads in flight first.
+template <typename T>
+__device__ __forceinline__ void stage_transposed_cg(const T* g, int ld, T* s) {
+  T v[TILE_PER_THREAD];
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) {
+    const int e = threadIdx.x + q * THREADS;
+    v[q] = ldcg(g + (size_t)(e >> 6) * ld + (e & 63));
+  }
+#pragma unroll
+  for (int q = 0; q < TILE_PER_THREAD; ++q) {
+    const int e = threadIdx.x + q * THREADS;
+    s[(e & 63) * LDA + (e >> 6)] = v[q];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void acc_to_smem_transposed(const T acc[16], T* s) {
+#pragma unroll
+  for (int rs = 0; rs < 2; ++rs)
+#pragma unroll
+    for (int cs = 0; cs < 8; ++cs) s[acc_col(cs) * LDA + acc_row(rs)] = acc[TileMMA<T>::idx(rs, cs)];
+}
+
+// XG(i, j, k) for rows i .. i+rows-1 (rows <= 2).  Shared memory: three tiles.
+template <typename T>
+__device__ void inverse_update(const DFArgs& a, int i, int rows, int j, int k, T* s) {
+  T* sB = s;
+  T* sA0 = s + NB * LDA;
+  T* sA1 = s + 2 * NB * LDA;
+  stage_async(tile<T>(a, i, k), a.ld, sA0, LDA);
+  if (rows > 1) stage_async(tile<T>(a, i + 1, k), a.ld, sA1, LDA);
+  T acc0[16], acc1[16];
+  if (k > j) {
+    load_acc(xtile_out<T>(a, i, j), a.ld, acc0);
+    if (rows > 1) load_acc(xtile_out<T>(a, i + 1, j), a.ld, acc1);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc0[e] = acc1[e] = T(0);
+  }
+  stage_transposed_cg<T>(xtile<T>(a, k, j), k == j ? NB : a.ld, sB);  // X_kj^T
+  cp_async_wait_all();
+  __syncthreads();
+  TileMMA<T>::sub(sA0, sB, acc0);
+  if (rows > 1) TileMMA<T>::sub(sA1, sB, acc1);
+  store_acc(xtile_out<T>(a, i, j), a.ld, acc0);
+  if (rows > 1) store_acc(xtile_out<T>(a, i + 1, j), a.ld, acc1);
+}
+
+// XZ(i, j).  Shared memory: three tiles.
+template <typename T>
+__device__ void inverse_finish(const DFArgs& a, int i, int j, T* s) {
+  T* sB = s;
+  T* sA = s + NB * LDA;
+  T* sX = s + 2 * NB * LDA;
+  stage_async(tile<T>(a, i, i - 1), a.ld, sA, LDA);
+  stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)i * NB * NB, NB, sX, LDA);  // X_ii
+  T acc[16];
+  if (i - 1 > j) {
+    load_acc(xtile_out<T>(a, i, j), a.ld, acc);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  }
+  stage_transposed_cg<T>(xtile<T>(a, i - 1, j), i - 1 == j ? NB : a.ld, sB);  // X_{i-1,j}^T
+  cp_async_wait_all();
+  __syncthreads();
+  TileMMA<T>::sub(sA, sB, acc);  // V_ij complete
+  __syncthreads();
+  acc_to_smem_transposed(acc, sB);  // V^T
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = T(0);
+  TileMMA<T>::sub(sX, sB, acc);  // -X_ii V
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
+  store_acc(xtile_out<T>(a, i, j), a.ld, acc);
+}
+
+// The worker CTAs' task loop.  FP32 lists (T = float): every update task
+// (one to four rows) runs on the tcgen05 tensor cores (update_rows_tc, w
+// holds the CTA's TMEM); FP64 lists: DMMA tile products.
+template <typename T>
+__device__ void df_worker_loop(const DFArgs& a, unsigned char* smem, int* s_task_p, int* s_ok_p, TcWorker* w) {
+  int& s_task = *s_task_p;
+  int& s_ok = *s_ok_p;
   T* sA = reinterpret_cast<T*>(smem);
   T* sB = sA + NB * LDA;
   const int nt = a.nt;
@@ -1331,7 +1525,47 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
     TRACE(0, t);
     TRACE(3, t);
     T acc[16];
-    if (type == TASK_I) {
+    if (sizeof(T) == 4 && (type == TASK_U || type == TASK_U2 || type == TASK_U3 || type == TASK_U4)) {
+      // U(i + r, j, k), r < rows: L_(i+r)k, L_jk final and the k previous updates of each (i + r, j)
+      const int rows = type == TASK_U ? 1 : type == TASK_U2 ? 2 : type == TASK_U3 ? 3 : 4;
+      const int* fl[9];
+      int tg[9];
+      fl[0] = a.fin + j * nt + k;
+      tg[0] = 1;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int rr = r < rows ? r : 0;
+        fl[1 + 2 * r] = a.fin + (i + rr) * nt + k;
+        tg[1 + 2 * r] = 1;
+        fl[2 + 2 * r] = a.upd + (i + rr) * nt + j;
+        tg[2 + 2 * r] = k;
+      }
+      if (!wait_all(a, fl, tg, 1 + 2 * rows, &s_ok)) return;
+      TRACE(1, t);
+      if (!update_rows_tc(a, i, rows, j, k, *w)) return;
+      if (threadIdx.x < rows) st_release(a.upd + (i + threadIdx.x) * nt + j, k + 1);
+      TRACE(2, t);
+    } else if (type == TASK_XG) {
+      const int rows = i + 1 < nt ? 2 : 1;
+      const int* fl[5] = {k == j ? a.fin + j * nt + j : a.xfin + k * nt + j, a.fin + i * nt + k,
+                          a.xupd + i * nt + j, a.fin + (i + rows - 1) * nt + k, a.xupd + (i + rows - 1) * nt + j};
+      const int tg[5] = {k == j ? 2 : 1, 1, k - j, 1, k - j};
+      if (!wait_all(a, fl, tg, 5, &s_ok)) return;
+      TRACE(1, t);
+      inverse_update<T>(a, i, rows, j, k, sA);
+      __syncthreads();
+      if (threadIdx.x < rows) st_release(a.xupd + (i + threadIdx.x) * nt + j, k - j + 1);
+      TRACE(2, t);
+    } else if (type == TASK_XZ) {
+      const int* fl[4] = {a.fin + i * nt + i - 1, i - 1 == j ? a.fin + j * nt + j : a.xfin + (i - 1) * nt + j,
+                          a.fin + i * nt + i, a.xupd + i * nt + j};
+      const int tg[4] = {1, i - 1 == j ? 2 : 1, 2, i - 1 - j};
+      if (!wait_all(a, fl, tg, 4, &s_ok)) return;
+      TRACE(1, t);
+      inverse_finish<T>(a, i, j, sA);
+      publish(a.xfin + i * nt + j, 1);
+      TRACE(2, t);
+    } else if (type == TASK_I) {
       // I(k): inv(L_kk) for the solves of column k, from the stored L_kk
       if (!wait_geq(a, a.fin + k * nt + k, 1, &s_ok)) return;
       TRACE(1, t);
@@ -1380,21 +1614,6 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
         st_release(a.upd + (i + 1) * nt + j, k + 1);
       }
       TRACE(2, t);
-    } else if (sizeof(T) == 4 && type == TASK_U3) {  // FP32 lists only: seven tiles of shared memory
-      const int* fl[7] = {a.fin + i * nt + k,       a.fin + (i + 1) * nt + k,       a.fin + (i + 2) * nt + k,
-                          a.fin + j * nt + k,       a.upd + i * nt + j,             a.upd + (i + 1) * nt + j,
-                          a.upd + (i + 2) * nt + j};
-      const int tg[7] = {1, 1, 1, 1, k, k, k};
-      if (!wait_all(a, fl, tg, 7, &s_ok)) return;
-      TRACE(1, t);
-      update_tile_triple(a, i, j, k, acc, sA);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        st_release(a.upd + i * nt + j, k + 1);
-        st_release(a.upd + (i + 1) * nt + j, k + 1);
-        st_release(a.upd + (i + 2) * nt + j, k + 1);
-      }
-      TRACE(2, t);
     } else {
       // S(i, j), i >= j + 2: the tile after its last update, times inv(L_jj)^T
       const int col = j;
@@ -1421,6 +1640,31 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   }
 }
 
+// F32CHAIN (FP32 matrices only): the chain CTA runs the FP32 chain
+// (run_chain_f32) and the task list has no I(k) tasks; otherwise run_chain,
+// whose diagonal tiles are factored in FP64.  The FP32 workers hold TMEM for
+// their tensor-core updates from start to end.
+template <typename T, bool F32CHAIN>
+__global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_task, s_ok;
+  if (blockIdx.x == 0) {
+    if constexpr (F32CHAIN) run_chain_f32(a, smem, &s_ok);
+    else run_chain<T>(a, smem, &s_ok);
+    return;
+  }
+  if constexpr (sizeof(T) == 4) {
+    __shared__ __align__(8) uint64_t s_mbar;
+    __shared__ uint32_t s_tmem;
+    TcWorker w;
+    tc_worker_begin(&s_mbar, &s_tmem, smem, 2, w);
+    df_worker_loop<T>(a, smem, &s_task, &s_ok, &w);
+    tc_worker_end(w);
+  } else {
+    df_worker_loop<T>(a, smem, &s_task, &s_ok, nullptr);
+  }
+}
+
 // Batched factorisation: every task comes from the shared list (there is no
 // chain CTA); F(k) applies its last update itself.  Shared memory: two T
 // tiles (sA, sB) for the updates and solves; F uses two FP64 tiles (L_kk,
@@ -1433,15 +1677,17 @@ constexpr size_t batch_smem_bytes() {
   else return std::max(factor_task_f32_smem_bytes(), 5 * NB * LDA * sizeof(T));
 }
 
-// Two CTAs per SM in the mixed path: a second task in flight per SM hides
-// L2 latency (measured 9.8 ms against 12.4 ms for a 256-replica step at one
-// CTA per SM).  The mixed path's F tasks factor and invert in FP32 like the
-// single-matrix FP32 chain.  One CTA per SM in the FP64 path.
+// The batched kernel's task loop.  The mixed path's F tasks factor and invert
+// in FP32 like the single-matrix FP32 chain.  Its updates stay 3xTF32
+// `mma.sync` products in pairs: with tcgen05 tasks (update_rows_tc, one row
+// pair per task) the 256-replica factorisation took 7.8 ms against 4.7 ms --
+// each task waits for its own MMAs and pays two memory round trips (operands,
+// then C), where the mma.sync task stages all five tiles in one round and
+// overlaps its loads with the math inside the CTA, and the batch runs two
+// CTAs per SM to hide what is left.
 template <typename T>
-__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
-                                                                 const int4* __restrict__ tasks, int ntasks,
-                                                                 int* ctl) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ void batch_worker_loop(const CholRep* __restrict__ reps, const int4* __restrict__ tasks, int ntasks,
+                                  int* ctl, unsigned char* smem) {
   __shared__ int s_task, s_ok;
   T* sA = reinterpret_cast<T*>(smem);
   T* sB = sA + NB * LDA;
@@ -1523,16 +1769,29 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
   }
 }
 
+// Two CTAs per SM in the mixed path: a second task in flight per SM hides
+// L2 latency (measured 9.8 ms against 12.4 ms for a 256-replica step at one
+// CTA per SM).  One CTA per SM in the FP64 path.
+template <typename T>
+__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
+                                                                 const int4* __restrict__ tasks, int ntasks,
+                                                                 int* ctl) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  batch_worker_loop<T>(reps, tasks, ntasks, ctl, smem);
+}
+
 std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
 // Task list of the worker CTAs for an nt x nt tile grid (see the file comment).
-// group: updates per task down a column (2, or 3 for the FP32 kernel);
+// group: updates per task down a column (2; 4 for the FP32 kernel, whose
+// updates run on the tcgen05 tensor cores); inverse: the tasks that form
+// X = inv(L) as well;
 // inv_tasks: the I(k) tasks that invert the diagonal tiles (left out when the
 // chain CTA stores the inverses itself).
-int get_task_table(int nt, int group, bool inv_tasks, const int4** out, int* count) {
+int get_task_table(int nt, int group, bool inv_tasks, bool inverse, const int4** out, int* count) {
   std::lock_guard<std::mutex> lk(g_task_mu);
-  const int key = (nt * 4 + group) * 2 + (inv_tasks ? 1 : 0);
+  const int key = ((nt * 8 + group) * 2 + (inv_tasks ? 1 : 0)) * 2 + (inverse ? 1 : 0);
   auto it = g_task_tables.find(key);
   if (it != g_task_tables.end()) {
     *out = it->second.first;
@@ -1555,10 +1814,19 @@ int get_task_table(int nt, int group, bool inv_tasks, const int4** out, int* cou
     // (rows grouped: U(i, jj, k), U(i+1, jj, k) [, U(i+2, jj, k)] share L_jj,k)
     for (int jj = k + 2; jj < nt; ++jj) {
       int i = jj;
-      if (group == 3)
+      if (group >= 4)
+        for (; i + 3 < nt; i += 4) t.push_back(make_int4(TASK_U4, i, jj, k));
+      if (group >= 3)
         for (; i + 2 < nt; i += 3) t.push_back(make_int4(TASK_U3, i, jj, k));
       for (; i + 1 < nt; i += 2) t.push_back(make_int4(TASK_U2, i, jj, k));
       if (i < nt) t.push_back(make_int4(TASK_U, i, jj, k));
+    }
+    if (inverse) {
+      // X = inv(L): row k+1 finished, then column k's contributions to the
+      // rows below (pairs of rows)
+      for (int j = 0; j <= k; ++j) t.push_back(make_int4(TASK_XZ, k + 1, j, 0));
+      for (int j = 0; j <= k; ++j)
+        for (int i = k + 2; i < nt; i += 2) t.push_back(make_int4(TASK_XG, i, j, k));
     }
   }
   int4* d = nullptr;
@@ -1577,15 +1845,19 @@ int get_task_table(int nt, int group, bool inv_tasks, const int4** out, int* cou
 
 template <typename T, bool F32CHAIN>
 size_t df_smem_bytes() {
-  // the chain, or a grouped update (three in FP32, two in FP64)
+  // the chain, or a grouped update (the tensor-core operands in FP32, five
+  // tiles in FP64)
   return std::max(F32CHAIN ? chain_f32_smem_bytes() : chain_smem_bytes<T>(),
-                  (sizeof(T) == 4 ? 7 : 5) * NB * LDA * sizeof(T));
+                  sizeof(T) == 4 ? tc_worker_smem_bytes(2) : 5 * NB * LDA * sizeof(T));
 }
 
 // tasks_override / spin_limit: only for the wait-expiry self-test.
+// X (or null): also form X = inv(L) (off-diagonal tiles); ints then holds
+// the X flags after the factorisation's.
 template <typename T, bool F32CHAIN = false>
 int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned* err, cudaStream_t st,
-              const int4* tasks_override = nullptr, int ntasks_override = 0, long long spin_limit = SPIN_LIMIT) {
+              const int4* tasks_override = nullptr, int ntasks_override = 0, long long spin_limit = SPIN_LIMIT,
+              T* X = nullptr) {
   static_assert(!F32CHAIN || sizeof(T) == 4, "the FP32 chain factors FP32 matrices");
   const int nt = ld / NB;
   const int4* tasks = nullptr;
@@ -1594,7 +1866,7 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
     tasks = tasks_override;
     ntasks = ntasks_override;
   } else {
-    int rc = get_task_table(nt, sizeof(T) == 4 ? 3 : 2, !F32CHAIN, &tasks, &ntasks);
+    int rc = get_task_table(nt, sizeof(T) == 4 ? 4 : 2, !F32CHAIN, X != nullptr, &tasks, &ntasks);
     if (rc) return rc;
   }
   const size_t smem = df_smem_bytes<T, F32CHAIN>();
@@ -1616,7 +1888,7 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
   // one CTA per SM: the chain CTA has its SM to itself
   int grid = num_sms;
   if (grid > ntasks + 1) grid = ntasks + 1;  // the chain CTA plus the shared tasks
-  PBG_CUDA_TRY(cudaMemsetAsync(ints, 0, (3 + 2 * (size_t)nt * nt) * sizeof(int), st));
+  PBG_CUDA_TRY(cudaMemsetAsync(ints, 0, (3 + (X ? 4 : 2) * (size_t)nt * nt) * sizeof(int), st));
   PBG_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
   DFArgs args;
   args.A = A;
@@ -1628,6 +1900,9 @@ int launch_df(T* A, int n, int ld, int* info, void* invdiag, int* ints, unsigned
   args.ctl = ints;
   args.upd = ints + 3;
   args.fin = ints + 3 + nt * nt;
+  args.X = X;
+  args.xupd = ints + 3 + 2 * nt * nt;
+  args.xfin = ints + 3 + 3 * nt * nt;
   args.info = info;
   args.invdiag = invdiag;
   args.err = err;
@@ -1663,7 +1938,7 @@ extern "C" __attribute__((visibility("default"))) int pbg_selftest_wait_expiry(l
   if (spin_limit < 1 || spin_limit > (1LL << 24)) return PBG_ERR_ARG;
   const int4* full = nullptr;
   int nfull = 0;
-  int rc = get_task_table(nt, 2, true, &full, &nfull);
+  int rc = get_task_table(nt, 2, true, false, &full, &nfull);
   if (rc) return rc;
   std::vector<int4> tasks(nfull);
   PBG_CUDA_TRY(cudaMemcpy(tasks.data(), full, nfull * sizeof(int4), cudaMemcpyDeviceToHost));
@@ -1742,7 +2017,7 @@ extern "C" __attribute__((visibility("default"))) int pbg_chain_trace(long long*
 // error word.
 size_t df_work_bytes(int ld) {
   const int nt = ld / NB;
-  return (3 + 2 * (size_t)nt * nt + 1) * sizeof(int) + 64;
+  return (3 + 4 * (size_t)nt * nt + 1) * sizeof(int) + 64;
 }
 
 // Factors A in place and writes the inverse of every diagonal factor tile to
@@ -1750,17 +2025,23 @@ size_t df_work_bytes(int ld) {
 // factorisation use them, and so do the SPD inverse and the triangular solve
 // of the midpoint scheme).  Both A and invdiag start on 16-byte boundaries.
 int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,
-                       cudaStream_t st) {
+                       cudaStream_t st, void* X) {
   const int nt = ld / NB;
   if (reinterpret_cast<uintptr_t>(A) % 16 != 0 || reinterpret_cast<uintptr_t>(invdiag) % 16 != 0) {
     pbg_set_error_message("cholesky: the matrix and its workspace must start on 16-byte boundaries");
     return PBG_ERR_ARG;
   }
   int* ints = static_cast<int*>(work);
-  unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 2 * (size_t)nt * nt);
-  if (precision == PBG_PREC_FP64) return launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st);
+  unsigned* err = reinterpret_cast<unsigned*>(ints + 3 + 4 * (size_t)nt * nt);
+  if (precision == PBG_PREC_FP64)
+    return launch_df<double>((double*)A, n, ld, info, invdiag, ints, err, st, nullptr, 0, SPIN_LIMIT, (double*)X);
   if (precision == PBG_PREC_MIXED_FP64_DIAG)
-    return launch_df<float, false>((float*)A, n, ld, info, invdiag, ints, err, st);
+    return launch_df<float, false>((float*)A, n, ld, info, invdiag, ints, err, st, nullptr, 0, SPIN_LIMIT,
+                                   (float*)X);
+  if (X) {
+    pbg_set_error_message("cholesky: X = inv(L) is formed with FP64 or FP64-diagonal factorisations only");
+    return PBG_ERR_ARG;
+  }
   return launch_df<float, true>((float*)A, n, ld, info, invdiag, ints, err, st);
 }
 
@@ -1843,9 +2124,10 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
 
 
 // ---------------------------------------------------------------- SPD inverse on the tensor cores
-// inv(A) = X^T X with A = L L^T (the data-flow factorisation above) and
-// X = inv(L): X level by level, joining pairs of finished diagonal blocks
-// (1 + 2 ceil(log2 nt) launches) -- and X^T X with one CTA per lower tile.  Every tile product is
+// inv(A) = X^T X with A = L L^T and X = inv(L): the data-flow factorisation
+// forms X's off-diagonal tiles in the same launch (XG / XZ tasks), then X's
+// diagonal tiles are copied from invdiag and X^T X runs with one CTA per lower
+// tile.  Every tile product is
 // TileMMA: FP64 DMMA for FP64 matrices, 3xTF32 split products with FP32
 // accumulation for FP32 ones.  Used by the SPD inverse of the FP64
 // lubrication path (cholesky.cu) and by the mixed lubricated path, which also
@@ -1887,31 +2169,6 @@ __device__ __forceinline__ void stage_transposed(const T* __restrict__ g, int ld
   store_tile_transposed(v, s);
 }
 
-// inv(L) level by level (recursive doubling on the block structure): with
-// the diagonal tiles X_kk = inv(L_kk) in place, level s joins pairs of
-// finished diagonal blocks A = [2bs, 2bs+s) and C = [2bs+s, 2bs+2s) (tiles):
-//   inv([L_AA 0; L_CA L_CC]) = [X_AA 0; -X_CC L_CA X_AA, X_CC],
-// as two launches -- U = -L_CA X_AA, then X_CA = X_CC U -- so the whole
-// inverse takes 1 + 2 ceil(log2 nt) launches with no waits between CTAs.  U
-// lives in the (unused) upper triangle of X: U_ij at tile (a0+j, c0+i).
-
-// The tile of level s that CTA `idx` computes: pair (a0, c0), C row i, A
-// column j; false beyond the last tile.
-__device__ __forceinline__ bool level_tile(int nt, int s, int idx, int& a0, int& c0, int& i, int& j) {
-  for (int b = 0;; ++b) {
-    a0 = 2 * b * s;
-    c0 = a0 + s;
-    if (c0 >= nt) return false;
-    const int cnt = min(s, nt - c0) * s;
-    if (idx < cnt) {
-      i = idx / s;
-      j = idx % s;
-      return true;
-    }
-    idx -= cnt;
-  }
-}
-
 // X_kk = inv(L_kk), upper triangle zero (one CTA per diagonal tile).
 template <typename T>
 __global__ void __launch_bounds__(THREADS) trtri_diag_kernel(const T* __restrict__ invdiag, T* X, int ld) {
@@ -1926,69 +2183,6 @@ __global__ void __launch_bounds__(THREADS) trtri_diag_kernel(const T* __restrict
     const int e = threadIdx.x + q * THREADS, r = e >> 6, c = e & 63;
     g[(size_t)r * ld + c] = c <= r ? v[q] : T(0);
   }
-}
-
-// Level s, first half: U_ij = -sum_{k=j}^{s-1} L_{c0+i, a0+k} X_{a0+k, a0+j}
-// (X_AA lower), stored at tile (a0+j, c0+i).
-template <typename T>
-__global__ void __launch_bounds__(THREADS) trtri_level_u_kernel(const T* __restrict__ L, T* X, int ld, int nt,
-                                                                int s) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* sA = reinterpret_cast<T*>(smem);
-  T* sB = sA + NB * LDA;
-  int a0, c0, i, j;
-  if (!level_tile(nt, s, blockIdx.x, a0, c0, i, j)) return;
-  const int ci = c0 + i, aj = a0 + j;
-  T acc[16];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) acc[e] = T(0);
-  T vb[TILE_PER_THREAD];
-  load_tile_regs(X + (size_t)(a0 + j) * NB * ld + (size_t)aj * NB, ld, vb);
-  for (int k = j; k < s; ++k) {
-    stage_async(L + (size_t)ci * NB * ld + (size_t)(a0 + k) * NB, ld, sA, LDA);
-    store_tile_transposed(vb, sB);
-    if (k + 1 < s) load_tile_regs(X + (size_t)(a0 + k + 1) * NB * ld + (size_t)aj * NB, ld, vb);
-    cp_async_wait_all();
-    __syncthreads();
-    TileMMA<T>::sub(sA, sB, acc);
-    __syncthreads();
-  }
-  store_acc(X + (size_t)aj * NB * ld + (size_t)ci * NB, ld, acc);
-}
-
-// Level s, second half: X_{c0+i, a0+j} = sum_{k=0}^{i} X_{c0+i, c0+k} U_kj.
-template <typename T>
-__global__ void __launch_bounds__(THREADS) trtri_level_x_kernel(T* X, int ld, int nt, int s) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* sA = reinterpret_cast<T*>(smem);
-  T* sB = sA + NB * LDA;
-  int a0, c0, i, j;
-  if (!level_tile(nt, s, blockIdx.x, a0, c0, i, j)) return;
-  const int ci = c0 + i, aj = a0 + j;
-  T acc[16];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) acc[e] = T(0);
-  T vb[TILE_PER_THREAD];
-  load_tile_regs(X + (size_t)aj * NB * ld + (size_t)c0 * NB, ld, vb);
-  for (int k = 0; k <= i; ++k) {
-    stage_async(X + (size_t)ci * NB * ld + (size_t)(c0 + k) * NB, ld, sA, LDA);
-    store_tile_transposed(vb, sB);
-    if (k < i) load_tile_regs(X + (size_t)aj * NB * ld + (size_t)(c0 + k + 1) * NB, ld, vb);
-    cp_async_wait_all();
-    __syncthreads();
-    TileMMA<T>::sub(sA, sB, acc);  // acc = -X_CC U
-    __syncthreads();
-  }
-#pragma unroll
-  for (int e = 0; e < 16; ++e) acc[e] = -acc[e];
-  store_acc(X + (size_t)ci * NB * ld + (size_t)aj * NB, ld, acc);
-}
-
-// Tiles of level s (host side of level_tile).
-inline int level_tiles(int nt, int s) {
-  int n = 0;
-  for (int c0 = s; c0 < nt; c0 += 2 * s) n += std::min(s, nt - c0) * s;
-  return n;
 }
 
 // out_IJ = scale (X^T X)_IJ = scale sum_{k >= I} X_kI^T X_kJ for the lower
@@ -2071,26 +2265,7 @@ __global__ void b_invdiag_kernel(const T* __restrict__ G, int ld, int nt, T inv_
 template <typename T>
 int set_tc_smem() {
   constexpr int smem = (int)tc_smem_bytes<T>();
-  PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_level_u_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  PBG_CUDA_TRY(cudaFuncSetAttribute(trtri_level_x_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   PBG_CUDA_TRY(cudaFuncSetAttribute(lauum_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  return PBG_OK;
-}
-
-template <typename T>
-int trtri_tc(const T* L, const T* invdiag, T* X, int ld, cudaStream_t st) {
-  const int nt = ld / NB;
-  constexpr size_t smem = tc_smem_bytes<T>();
-  if (int rc = set_tc_smem<T>()) return rc;
-  trtri_diag_kernel<T><<<nt, THREADS, 0, st>>>(invdiag, X, ld);
-  PBG_CHECK_LAUNCH();
-  for (int s = 1; s < nt; s *= 2) {
-    const int tiles = level_tiles(nt, s);
-    trtri_level_u_kernel<T><<<tiles, THREADS, smem, st>>>(L, X, ld, nt, s);
-    PBG_CHECK_LAUNCH();
-    trtri_level_x_kernel<T><<<tiles, THREADS, smem, st>>>(X, ld, nt, s);
-    PBG_CHECK_LAUNCH();
-  }
   return PBG_OK;
 }
 
@@ -2106,10 +2281,13 @@ int lauum_tc(const T* X, int ld, T scale, bool reversed, T* out, cudaStream_t st
 
 }  // namespace
 
-int launch_trtri_tc(const void* L, const void* invdiag, void* X, int ld, int precision, cudaStream_t st) {
+int launch_trtri_diag(const void* invdiag, void* X, int ld, int precision, cudaStream_t st) {
   if (ld % NB != 0 || ld <= 0) return PBG_ERR_ARG;
-  if (precision == PBG_PREC_FP64) return trtri_tc<double>((const double*)L, (const double*)invdiag, (double*)X, ld, st);
-  return trtri_tc<float>((const float*)L, (const float*)invdiag, (float*)X, ld, st);
+  const int nt = ld / NB;
+  if (precision == PBG_PREC_FP64) trtri_diag_kernel<double><<<nt, THREADS, 0, st>>>((const double*)invdiag, (double*)X, ld);
+  else trtri_diag_kernel<float><<<nt, THREADS, 0, st>>>((const float*)invdiag, (float*)X, ld);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
 }
 
 int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* out, int precision, cudaStream_t st) {
@@ -2145,9 +2323,10 @@ int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st) {
     pbg_set_error_message("tensor-core inverse: misaligned workspace");
     return PBG_ERR_ARG;
   }
-  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED_FP64_DIAG, info, w.invdiag, w.scratch, st);
+  // the factorisation forms X's off-diagonal tiles in the same launch
+  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED_FP64_DIAG, info, w.invdiag, w.scratch, st, w.X);
   if (rc != PBG_OK) return rc;
-  return trtri_tc<float>(w.F, w.invdiag, w.X, ld, st);
+  return launch_trtri_diag(w.invdiag, w.X, ld, PBG_PREC_MIXED, st);
 }
 
 int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, cudaStream_t st) {

@@ -165,7 +165,7 @@ __device__ __forceinline__ void smith_pair(T sx, T sy, T sz, T cO, T cQ, T alpha
 
 // One 16 x 16 bead tile (I, J), I >= J, of the tensor described by `a`.
 template <typename T>
-__device__ __forceinline__ void rpy_tile_body(const RpyArgs& a, int I, int J) {
+__device__ __forceinline__ void rpy_tile_body(const RpyArgs& a, int I, int J, void* M_lower) {
   using V2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // layout: out tile [TV][TV+1] T | recip table [n_recip][8] T | real [n_real][4] double |
@@ -273,7 +273,7 @@ __device__ __forceinline__ void rpy_tile_body(const RpyArgs& a, int I, int J) {
   T* M = reinterpret_cast<T*>(a.M);
   const int n3 = 3 * n;
   const int row0 = 3 * I * TB, col0 = 3 * J * TB;
-  T* ML = reinterpret_cast<T*>(a.M_lower);
+  T* ML = reinterpret_cast<T*>(M_lower);
   for (int t = tid; t < TV * TV; t += THREADS) {
     const int r = t / TV, c = t % TV;
     if (row0 + r < n3 && col0 + c < n3) {
@@ -298,15 +298,16 @@ __global__ void __launch_bounds__(THREADS) rpy_tile_kernel(RpyArgs a) {
   while ((I + 1) * (I + 2) / 2 <= b) ++I;
   while (I * (I + 1) / 2 > b) --I;
   const int J = b - I * (I + 1) / 2;
-  rpy_tile_body<T>(a, I, J);
+  rpy_tile_body<T>(a, I, J, a.M_lower);
 }
 
-// Batched build: block b computes tile (work[b].y, work[b].z) of replica work[b].x.
+// Batched build: block b computes tile (work[b].y, work[b].z) of replica work[b].x;
+// with fill_lower the lower block triangle also goes to the replica's M_lower.
 template <typename T>
 __global__ void __launch_bounds__(THREADS) rpy_batch_kernel(const RpyArgs* __restrict__ args,
-                                                            const int4* __restrict__ work) {
+                                                            const int4* __restrict__ work, int fill_lower) {
   const int4 w = work[blockIdx.x];
-  rpy_tile_body<T>(args[w.x], w.y, w.z);
+  rpy_tile_body<T>(args[w.x], w.y, w.z, fill_lower ? args[w.x].M_lower : nullptr);
 }
 
 __global__ void positions_from_pairs_kernel(const double* __restrict__ pairs, int n, double* __restrict__ pos) {
@@ -574,7 +575,7 @@ int launch_rpy_tensor(const PairSource& src, const double* pos, const double* ra
 size_t rpy_batch_arg_bytes() { return sizeof(RpyArgs); }
 
 void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool smith, const EwaldTables* t,
-                   double scale, void* M, int ld, void* phase, void* dst) {
+                   double scale, void* M, void* M_lower, int ld, void* phase, void* dst) {
   RpyArgs a{};
   a.src.pos = pos;
   a.src.pairs = nullptr;
@@ -582,7 +583,7 @@ void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool
   a.src.L = L;
   a.radii = radii;
   a.M = M;
-  a.M_lower = nullptr;
+  a.M_lower = M_lower;
   a.L = L;
   a.scale = scale;
   a.n = n;
@@ -611,9 +612,11 @@ void rpy_batch_work(int replica, int n, std::vector<int4>& work) {
 }
 
 // args: device array of the replicas' argument blocks (rpy_batch_arg);
-// the phase tables are built first (one grid row per replica).
+// the phase tables are built first (one grid row per replica).  fill_lower:
+// each replica's lower block triangle also goes to its M_lower (the matrix
+// the step factors next).
 int launch_rpy_batch(int precision, bool smith, const EwaldTables* t, const void* args, const int4* work,
-                     int nwork, int n_replicas, cudaStream_t st) {
+                     int nwork, int n_replicas, bool fill_lower, cudaStream_t st) {
   if (nwork <= 0) return PBG_OK;
   const RpyArgs* a = static_cast<const RpyArgs*>(args);
   if (smith && t && t->n_recip > 0 && n_replicas > 0) {
@@ -629,10 +632,10 @@ int launch_rpy_batch(int precision, bool smith, const EwaldTables* t, const void
   }
   if (precision == PBG_PREC_FP64) {
     PBG_CUDA_TRY(cudaFuncSetAttribute(rpy_batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    rpy_batch_kernel<double><<<nwork, THREADS, smem, st>>>(a, work);
+    rpy_batch_kernel<double><<<nwork, THREADS, smem, st>>>(a, work, fill_lower ? 1 : 0);
   } else {
     PBG_CUDA_TRY(cudaFuncSetAttribute(rpy_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    rpy_batch_kernel<float><<<nwork, THREADS, smem, st>>>(a, work);
+    rpy_batch_kernel<float><<<nwork, THREADS, smem, st>>>(a, work, fill_lower ? 1 : 0);
   }
   PBG_CHECK_LAUNCH();
   return PBG_OK;

@@ -128,15 +128,17 @@ size_t cholesky_work_bytes(int ld, int precision);
 int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st);
 // cholesky_df.cu
 size_t df_work_bytes(int ld);
+// X (FP64 or FP64-diagonal factorisations): the same launch also forms the
+// off-diagonal tiles of X = inv(L) (ld x ld, lower; launch_trtri_diag copies
+// the diagonal ones from invdiag).
 int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,
-                       cudaStream_t st);
+                       cudaStream_t st, void* X = nullptr);
 size_t spd_inverse_work_bytes(int ld);
 int launch_spd_inverse(double* A, int n, int ld, int* info, void* work, cudaStream_t st);
 
-// X = inv(L) (L lower with its inverted diagonal tiles in invdiag) and
-// out = scale X^T X (optionally with every index i -> ld-1-i), on the tensor
-// cores, FP64 or FP32 (cholesky_df.cu).
-int launch_trtri_tc(const void* L, const void* invdiag, void* X, int ld, int precision, cudaStream_t st);
+// X's diagonal tiles from invdiag, and out = scale X^T X (optionally with
+// every index i -> ld-1-i), on the tensor cores, FP64 or FP32 (cholesky_df.cu).
+int launch_trtri_diag(const void* invdiag, void* X, int ld, int precision, cudaStream_t st);
 int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* out, int precision, cudaStream_t st);
 // SPD inverse of the mixed lubricated path (FP32).  The caller puts the
 // matrix (order ld, padded) in F; tc_factor_invert factors it in place
@@ -177,11 +179,12 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
 // Batched RPY / Smith-Ewald tensor build: one argument block per replica and
 // a work list of bead tiles (x = replica, y = I, z = J with I >= J).
 size_t rpy_batch_arg_bytes();
-// Fills the argument block of one replica into `dst` (rpy_batch_arg_bytes() bytes).
+// Fills the argument block of one replica into `dst` (rpy_batch_arg_bytes() bytes);
+// M_lower: the matrix that receives the lower block triangle when a launch asks for it.
 void rpy_batch_arg(const double* pos, const double* radii, int n, double L, bool smith, const EwaldTables* t,
-                   double scale, void* M, int ld, void* phase, void* dst);
+                   double scale, void* M, void* M_lower, int ld, void* phase, void* dst);
 void rpy_batch_work(int replica, int n, std::vector<int4>& work);
 int launch_rpy_batch(int precision, bool smith, const EwaldTables* t, const void* args, const int4* work,
-                     int nwork, int n_replicas, cudaStream_t st);
+                     int nwork, int n_replicas, bool fill_lower, cudaStream_t st);
 
 }  // namespace pbg

@@ -11,9 +11,9 @@ configuration (order 3 x beads, padded to a multiple of 64); `smith` builds it;
 `batch` advances a batch of replicas (N uniform in [32, 512], seed 1) by one
 step; `lub` takes one midpoint step of a lubricated box (rpy_smith_lub,
 radius 20, volume fraction 0.30, cutoff 0.5, Cichocki, m = 100, dt 0.1);
-`forces` steps a box of bonded chains (16 beads each, harmonic bonds and
-angles, Lennard-Jones 6-12, rpy_smith, Ermak, dt 0.05), so that the force
-kernels run every step.
+`forces` steps a box of bonded chains (16 beads each, bond angles at their
+150-degree equilibrium, harmonic bonds and angles, Lennard-Jones 6-12,
+rpy_smith, Ermak, dt 0.05), so that the force kernels run every step.
 Each case runs `--reps` times after one warm-up and prints the mean CUDA-event
 time of one launch; `--reps 0` runs the warm-up call only (a batch's first
 step is made of direct kernel launches, the later ones replay a CUDA graph).
@@ -148,30 +148,44 @@ def _lub(a, torch):
 
 
 def _chains(n_beads, length=16, seed=0):
-    """Straight chains of beads (radius 2, spacing 4.2 A) along random
-    directions in a box at about 2 % volume fraction, bonded along each chain
-    (rest length 4.2, k 5) with angle terms (150 degrees, k 2)."""
+    """Chains of beads (radius 2, bond length 4.2 A, every bond angle at its
+    150-degree equilibrium, random dihedrals) in a box at about 2 % volume
+    fraction, bonded along each chain (rest length 4.2, k 5) with angle terms
+    (150 degrees, k 2).  No three consecutive beads are collinear: the
+    harmonic angle force divides by sin(angle), which vanishes at 180 degrees."""
     from .bead import Bead
     rng = np.random.default_rng(seed)
     n_chains = max(1, n_beads // length)
     L = (n_chains * length * 4.0 / 3.0 * math.pi * 8.0 / 0.02) ** (1.0 / 3.0)
+    turn = math.radians(180.0 - 150.0)
     beads, pts_all = [], []
+
+    def walk():
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        pts = [rng.uniform(-L / 2, L / 2, 3)]
+        for _ in range(length - 1):
+            w = rng.normal(size=3)
+            w -= (w @ u) * u
+            w /= np.linalg.norm(w)
+            if len(pts) > 1:
+                u = math.cos(turn) * u + math.sin(turn) * w
+            pts.append(pts[-1] + 4.2 * u)
+        return pts
+
+    def clear(p, others):
+        for q in others:
+            d = p - q
+            d -= L * np.round(d / L)
+            if d @ d <= 4.5 ** 2:
+                return False
+        return True
+
     for c in range(n_chains):
         while True:
-            start = rng.uniform(-L / 2, L / 2, 3)
-            u = rng.normal(size=3)
-            u /= np.linalg.norm(u)
-            pts = [start + 4.2 * i * u for i in range(length)]
-            ok = True
-            for p in pts:
-                for q in pts_all:
-                    d = p - q
-                    d -= L * np.round(d / L)
-                    if d @ d <= 4.5 ** 2:
-                        ok = False
-                        break
-                if not ok:
-                    break
+            pts = walk()
+            ok = all(clear(p, pts[:max(0, i - 1)]) for i, p in enumerate(pts))
+            ok = ok and all(clear(p, pts_all) for p in pts)
             if ok:
                 break
         base = len(beads) + 1

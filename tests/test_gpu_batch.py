@@ -186,9 +186,9 @@ def test_alone_equals_mix_with_changing_membership():
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_autotuned_schedule_changes_no_result(precision):
-    """The schedule autotuner (merge order of the replicas' task segments x
-    CTAs per SM) times every candidate on the current matrices and keeps the
-    fastest; trajectories with the tuned schedule, and with each fixed
+    """The schedule autotuner (merge order of the replicas' task segments,
+    L2-sized chunks of replicas included, x CTAs per SM) times every
+    candidate on the current matrices and keeps the fastest; trajectories with the tuned schedule, and with each fixed
     schedule, are bit-identical to the default one."""
     from pybrown_b200.batch import ReplicaBatch
     configs = [_config(500 + k, N, 0.05, 10.0, 30.0) for k, N in enumerate((40, 130, 75, 200, 33))]
@@ -211,10 +211,11 @@ def test_autotuned_schedule_changes_no_result(precision):
     ref, _ = run(None)
     got, tuned = run("auto")
     assert np.array_equal(ref, got)
-    n_cand = 8 if precision == "mixed" else 4
+    n_orders = len(ReplicaBatch.MERGE_ORDERS)
+    n_cand = 2 * n_orders if precision == "mixed" else n_orders
     assert len(tuned["ms"]) == n_cand and all(v > 0 for v in tuned["ms"].values())
     assert tuned["ms"][(tuned["merge_order"], tuned["ctas_per_sm"])] == min(tuned["ms"].values())
-    for sched in (("replica_major", 1), ("smaller_first", 0), ("added", 1)):
+    for sched in (("replica_major", 1), ("smaller_first", 0), ("added", 1), ("chunk_32M", 0)):
         assert np.array_equal(ref, run(sched)[0]), sched
 
 

@@ -42,8 +42,10 @@ def test_cholesky_fp64(n):
     assert rel_err(np.tril(L), ref) <= 1e-12
 
 
-@pytest.mark.parametrize("n", [81, 192, 1000])
+@pytest.mark.parametrize("n", [3, 64, 81, 130, 192, 1000, 1536])
 def test_spd_inverse_fp64(n):
+    """inv(A) = X^T X with X = inv(L) formed inside the factorisation's task
+    list (one tile row for n <= 64: no inverse tasks; up to 24 x 24 tiles)."""
     A = _spd(n, 100 + n)
     X, info = _run("inv", A, n)
     assert info == 0
