@@ -323,11 +323,12 @@ def mixed_vs_oracle(pos, radii, seed, steps=5):
 
 
 # DRAM bytes (read + write) of one mixed factorisation of the N=1024 matrix,
-# from one ncu capture of the same kernel on the same order:
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:chol_df -c 1 --clock-control none \
-#       python -m pybrown_b200.profile_cases cholesky --order 3072 --precision mixed
-# (19,544,320 + 2,230,272 B); re-measure when the factorisation changes.
-CHOL_MIXED_TRAFFIC_BYTES = 19544320 + 2230272
+# from one ncu capture of the same kernel on the same order
+# (profiles/chol_df_mixed_order3072_full.md):
+#   ncu --set full --clock-control none -k regex:chol_df -s 1 -c 1 \
+#       python -m pybrown_b200.profile_cases cholesky --order 3072 --precision mixed --reps 1
+# (19,468,544 + 1,830,912 B); re-measure when the factorisation changes.
+CHOL_MIXED_TRAFFIC_BYTES = 19468544 + 1830912
 
 
 def replica_seed(rank):

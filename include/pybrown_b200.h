@@ -143,12 +143,15 @@ PBG_API int pbg_dev_check_overlaps(const double *pos, const double *radii, int n
 /* In-place lower Cholesky factor of an SPD matrix of order n (row-major,
  * leading dimension ld >= round_up(n, 64), rows/cols n..ld-1 are used as
  * padding).  precision selects FP64, the mixed FP32 path (float*; FP32
- * diagonal tiles, 3xTF32 trailing updates) or PBG_PREC_MIXED_FP64_DIAG.
+ * diagonal tiles, 3xTF32 trailing updates on the tcgen05 tensor cores) or
+ * PBG_PREC_MIXED_FP64_DIAG.  Replaces np.linalg.cholesky (box.py:554).
  * info_dev (int, device) receives 0 or 1 + the index of the first
  * non-positive pivot. */
 PBG_API int pbg_dev_cholesky(void *A, int n, int ld, int precision, int *info_dev, void *stream);
 
-/* In-place inverse of an SPD FP64 matrix via its Cholesky factor. */
+/* In-place inverse of an SPD FP64 matrix via its Cholesky factor: one
+ * data-flow launch factors A and forms X = inv(L), then X^T X.  Replaces
+ * np.linalg.inv (box.py:514,524,537). */
 PBG_API int pbg_dev_spd_inverse(double *A, int n, int ld, int *info_dev, void *stream);
 
 /* ---- system handle -------------------------------------------------- */
