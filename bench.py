@@ -163,7 +163,8 @@ class ClockSampler:
 
 class DeviceRun:
     """Device-resident stepping through the C ABI: state, D, B and the noise
-    pool live in HBM; one pbg_step_begin / attempt / end per step."""
+    pool live in HBM; one pbg_run call per step (from the second step one
+    CUDA graph launch, the move attempts under a device-side WHILE node)."""
 
     def __init__(self, pos, radii, precision, n_noise_steps, seed, torch, inp=None):
         from pybrown_b200 import _lib
@@ -175,21 +176,17 @@ class DeviceRun:
         rs = np.random.RandomState(seed)
         self.pool = torch.tensor(rs.normal(0.0, 1.0, size=(n_noise_steps + 64) * self.n), dtype=torch.float64,
                                  device="cuda")
-        self.cursor = 0
-        self.acc = _lib.ctypes.c_int(0)
+        self.cursor = 0  # draws consumed
+        self.j = 0
+        self.report = _lib.PbgStepReport()
 
     def step(self, dt):
         _lib, h = self._lib, self.box._h
-        _lib.call("pbg_step_begin", h, dt, 1, 1, 1, None)
-        while True:
-            if (self.cursor + 1) * self.n > self.pool.numel():
-                raise RuntimeError("noise pool exhausted")
-            xi = self.pool.data_ptr() + self.cursor * self.n * 8
-            self.cursor += 1
-            _lib.call("pbg_step_attempt", h, xi, _lib.ctypes.byref(self.acc), None)
-            if self.acc.value:
-                break
-        _lib.call("pbg_step_end", h, None)
+        base = self.pool.data_ptr() + 8 * self.cursor
+        _lib.call("pbg_run", h, self.j, 1, float(dt), 1, 1, 1, base, self.pool.numel() - self.cursor, None)
+        _lib.lib.pbg_run_report(h, _lib.ctypes.byref(self.report), None)
+        self.cursor += self.report.draws_consumed
+        self.j += 1
 
     def positions(self):
         out = np.empty(self.n)
@@ -521,7 +518,7 @@ def run_lub_section(args, torch, precisions=("fp64", "mixed")):
         ms = timed_steps(torch, lambda: run.step(w["dt"]), args.steps, flush)
         runs[prec] = run
         out[prec] = {"ms_per_step": ms / args.steps, "steps_per_s": args.steps / (ms * 1e-3),
-                     "move_attempts": run.cursor}
+                     "move_attempts": run.cursor // run.n}
     if "fp64" in runs and "mixed" in runs:
         d_ref = runs["fp64"].positions() - pos
         d_mix = runs["mixed"].positions() - pos

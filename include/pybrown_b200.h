@@ -302,8 +302,14 @@ PBG_API int pbg_step_finish(pbg_system *sys, double *pos_host, void *stream);
  * BD.py:177 (j % diff_freq == 0 ...), each step as Box.propagate does it.
  * Noise is consumed in order from `pool` (device or host, pool_len doubles);
  * each attempt takes 3N, so a pool filled from RandomState(seed) reproduces
- * the reference's trajectory.  The accept decision of each attempt
- * synchronises the stream, as pbg_step_attempt does.  A step that runs out of
+ * the reference's trajectory.  With a host pool (or the midpoint scheme,
+ * lubrication or the divergence term) the accept decision of each attempt
+ * synchronises the stream, as pbg_step_attempt does.  With a device pool and
+ * the Ermak scheme the attempts run on the device: from the second step with
+ * the same flags, dt and force state a step is one CUDA graph launch (its
+ * attempts under a conditional WHILE node) and one wait; the results are the
+ * same bit for bit.  Changing the system (pbg_set_state, pbg_set_immobile,
+ * pbg_set_interactions, pbg_set_divergence) drops that graph.  A step that runs out of
  * noise (PBG_ERR_NOISE) or of move attempts (PBG_ERR_ATTEMPTS, box.py:248)
  * is rolled back to its start positions and ends the run; pbg_run_report
  * gives the steps completed, the noise consumed and the attempt counts. */

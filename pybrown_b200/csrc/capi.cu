@@ -336,11 +336,13 @@ int pbg_destroy(pbg_system* sys) {
 
 int pbg_set_state(pbg_system* sys, const double* pos, const double* radii, const int* conn, void* stream) {
   if (!sys || !pos || !radii) return PBG_ERR_ARG;
+  pbg::drop_run_graph(sys);
   return pbg::system_set_state(sys, pos, radii, conn, (cudaStream_t)stream);
 }
 
 int pbg_set_divergence(pbg_system* sys, int on) {
   if (!sys) return PBG_ERR_ARG;
+  pbg::drop_run_graph(sys);
   return pbg::set_divergence(sys, on != 0);
 }
 
@@ -357,11 +359,13 @@ int pbg_set_positions(pbg_system* sys, const double* pos, void* stream) {
 int pbg_set_immobile(pbg_system* sys, int n_immobile, const double* pos, const double* radii, const int* order,
                      const int* conn_mi, void* stream) {
   if (!sys) return PBG_ERR_ARG;
+  pbg::drop_run_graph(sys);
   return pbg::set_immobile(sys, n_immobile, pos, radii, order, conn_mi, (cudaStream_t)stream);
 }
 
 int pbg_set_interactions(pbg_system* sys, const pbg_interactions* desc) {
   if (!sys) return PBG_ERR_ARG;
+  pbg::drop_run_graph(sys);
   return pbg::set_interactions(sys, desc);
 }
 

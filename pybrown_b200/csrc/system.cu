@@ -147,6 +147,11 @@ void destroy_system(pbg_system* s) {
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
   if (s->hpos) cudaFreeHost(s->hpos);
+  if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
+  if (s->d_run) cudaFree(s->d_run);
+  if (s->h_run) cudaFreeHost(s->h_run);
+  if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+  if (s->cap_stream2) cudaStreamDestroy(s->cap_stream2);
   delete s;
 }
 
@@ -744,6 +749,296 @@ int step_end(pbg_system* s, cudaStream_t st, double* pos_out) {
   return PBG_OK;
 }
 
+// ---- device-side steps of pbg_run -----------------------------------------
+// With the noise pool in device memory and the Ermak scheme (no lubrication,
+// no divergence term), a step runs
+// without the host between its attempts: the step start, then rounds of
+// {xi = the pool's next n draws, U = B xi, the move, the overlap test, the
+// undo of a rejected move, the bookkeeping} until a move is accepted, the
+// attempts reach max_move_attempts or the pool runs out, then the wrap.  The
+// same kernels run either one by one (the host reads the round's verdict) or,
+// from the second step with the same flags, dt and force state, as one CUDA
+// graph whose attempt rounds sit under a conditional WHILE node.  Every
+// arithmetic step is the host-driven one's, so the trajectories are equal bit
+// for bit.
+
+static bool device_accessible(const void* p);
+
+namespace {
+
+struct RunDev {
+  const double* pool;
+  long long pool_len;
+  long long used;  // draws consumed in this pbg_run call
+  int attempts;    // of the current step
+  int status;      // 0, RUN_NOISE or RUN_ATTEMPTS
+  int rounds;      // attempt rounds of the current step
+  int more;        // the current step's move was rejected and is tried again
+  int flags[4];    // the step's copy of dflags (overlap, factorisation infos)
+};
+constexpr int RUN_NOISE = 1, RUN_ATTEMPTS = 2;
+
+__global__ void run_step_init_kernel(RunDev* r) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    r->attempts = 0;
+    r->rounds = 0;
+    r->more = 1;
+  }
+}
+
+// xi = the pool's next n draws; zeros once the pool has run out (the move is
+// then nothing and the round ends the run).
+__global__ void run_gather_kernel(const RunDev* __restrict__ r, int n, double* __restrict__ xi) {
+  const long long used = r->used;
+  const bool ok = used + n <= r->pool_len;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    xi[i] = ok ? r->pool[used + i] : 0.0;
+}
+
+// The undo of a rejected move, pos += (U sqrt(2 dt)) * (-1): the arithmetic of
+// the host-driven undo (scale2 with mult = -1, then translate), each product
+// and sum rounded on its own (no contraction into an FMA).
+__global__ void run_undo_kernel(double* __restrict__ pos, const double* __restrict__ U, double s1, int n,
+                                const int* __restrict__ overlap) {
+  if (!*overlap) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pos[i] = __dadd_rn(pos[i], __dmul_rn(__dmul_rn(U[i], s1), -1.0));
+}
+
+// The round's bookkeeping: the draws consumed, the attempt counted, and
+// whether another round follows (the WHILE node's condition when captured).
+__global__ void run_round_update_kernel(RunDev* r, int n, int max_att, const int* __restrict__ overlap,
+                                        cudaGraphConditionalHandle handle, int use_handle) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int more = 0;
+  if (r->used + n > r->pool_len) {
+    r->status = RUN_NOISE;
+  } else {
+    r->used += n;
+    const int a = ++r->attempts;
+    if (*overlap) {
+      if (a >= max_att) r->status = RUN_ATTEMPTS;
+      else more = 1;
+    }
+  }
+  ++r->rounds;
+  r->more = more;
+  if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+}  // namespace
+
+// One round of attempts (six kernels and the overlap flag's reset).
+static int enqueue_run_round(pbg_system* s, cudaStream_t st, cudaGraphConditionalHandle handle, int use_handle) {
+  const int n = s->n;
+  RunDev* r = static_cast<RunDev*>(s->d_run);
+  run_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(r, n, s->xi);
+  PBG_CHECK_LAUNCH();
+  int rc = launch_trmv_lower(s->B, s->ld, n, s->prec, s->xi, s->U, st);
+  if (rc) return rc;
+  if ((rc = stochastic_step(s, 1.0, st))) return rc;
+  if ((rc = launch_overlap(s->pos, s->radii, s->N, s->p.box_length, s->p.overlap_treshold, s->conn, s->dflags,
+                           st)))
+    return rc;
+  if ((rc = overlap_immobile(s, s->dflags, st))) return rc;
+  run_undo_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->pos, s->U, std::sqrt(2 * s->dt), n, s->dflags);
+  PBG_CHECK_LAUNCH();
+  run_round_update_kernel<<<1, 32, 0, st>>>(r, n, std::max(1, s->p.max_move_attempts), s->dflags, handle,
+                                             use_handle);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+// The start of a step: the step-start snapshot of the positions, the matrices
+// and the deterministic move (step_begin), the round state.
+static int enqueue_run_start(pbg_system* s, double dt, int bDff, int bDnf, int chol, cudaStream_t st) {
+  const size_t pos_bytes = (size_t)s->N * 3 * sizeof(double);
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->pos_snap, s->pos, pos_bytes, cudaMemcpyDeviceToDevice, st));
+  int rc = step_begin(s, dt, bDff, bDnf, chol, st);
+  if (rc) return rc;
+  run_step_init_kernel<<<1, 32, 0, st>>>(static_cast<RunDev*>(s->d_run));
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+// The end of a step: the wrap and the step's report to pinned host memory.
+static int enqueue_run_tail(pbg_system* s, cudaStream_t st) {
+  int rc = launch_wrap(s->pos, s->n, s->p.box_length, st);
+  if (rc) return rc;
+  RunDev* r = static_cast<RunDev*>(s->d_run);
+  PBG_CUDA_TRY(cudaMemcpyAsync(r->flags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->h_run, s->d_run, sizeof(RunDev), cudaMemcpyDeviceToHost, st));
+  return PBG_OK;
+}
+
+void drop_run_graph(pbg_system* s) {
+  if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
+  s->run_exec = nullptr;
+  s->run_key = -1;
+}
+
+// Captures start + WHILE{round} + tail into s->run_exec.  A refusal by the
+// driver leaves run_refused set (steps then run their kernels one by one).
+static int capture_run_step(pbg_system* s, double dt, int bDff, int bDnf, int chol) {
+  if (!s->cap_stream) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+  if (!s->cap_stream2) PBG_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream2, cudaStreamNonBlocking));
+  const long long l0 = pbg_launch_count();
+  auto refuse = [&](cudaGraph_t g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    const long long k = pbg_launch_count() - l0;  // nothing ran
+    pbg_count_launches(-k);
+    pbg_count_host_calls(-k);
+    s->in_step = false;
+    s->run_refused = true;
+    return PBG_OK;
+  };
+  if (cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return refuse(nullptr);
+  int rc = enqueue_run_start(s, dt, bDff, bDnf, chol, s->cap_stream);
+  const long long fixed0 = pbg_launch_count() - l0;
+  bool ok = rc == PBG_OK;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle handle = 0;
+  cudaGraphNodeParams cp = {};
+  if (ok) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ok = cudaStreamGetCaptureInfo(s->cap_stream, &cs, nullptr, &g, &deps, &ndeps) == cudaSuccess &&
+         cs == cudaStreamCaptureStatusActive &&
+         cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t wnode = nullptr;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&wnode, g, deps, ndeps, &cp) == cudaSuccess &&
+           cudaStreamUpdateCaptureDependencies(s->cap_stream, &wnode, 1, cudaStreamSetCaptureDependencies) ==
+               cudaSuccess;
+    }
+    if (ok) {
+      ok = cudaStreamBeginCaptureToGraph(s->cap_stream2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed) == cudaSuccess;
+      if (ok) {
+        const long long r0 = pbg_launch_count();
+        rc = enqueue_run_round(s, s->cap_stream2, handle, 1);
+        s->run_round_kernels = pbg_launch_count() - r0;
+        cudaGraph_t body = nullptr;
+        ok = cudaStreamEndCapture(s->cap_stream2, &body) == cudaSuccess && rc == PBG_OK;
+      }
+    }
+  }
+  const long long before_tail = pbg_launch_count();
+  if (ok) ok = enqueue_run_tail(s, s->cap_stream) == PBG_OK;
+  const long long tail = pbg_launch_count() - before_tail;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(s->cap_stream, &graph);
+  if (!ok || end != cudaSuccess || !graph) return refuse(graph);
+  const cudaError_t inst = cudaGraphInstantiate(&s->run_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) {
+    s->run_exec = nullptr;
+    return refuse(nullptr);
+  }
+  s->run_fixed_kernels = fixed0 + tail;
+  const long long k = pbg_launch_count() - l0;  // nothing ran yet
+  pbg_count_launches(-k);
+  pbg_count_host_calls(-k);
+  s->in_step = false;  // the capture went through step_begin without running it
+  return PBG_OK;
+}
+
+// pbg_run's steps on the device (see above); the pool is device memory.
+// Outcomes and rollbacks are those of the host-driven loop below.
+static int run_device(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int lub_freq,
+                      int chol_freq, const double* pool, long long pool_len, cudaStream_t st) {
+  const size_t pos_bytes = (size_t)s->N * 3 * sizeof(double);
+  if (!s->d_run) {
+    if (cudaMalloc(&s->d_run, sizeof(RunDev)) != cudaSuccess) {
+      cudaGetLastError();
+      s->d_run = nullptr;
+      pbg_set_error_message("cudaMalloc of the run state failed");
+      return PBG_ERR_NOMEM;
+    }
+    if (cudaMallocHost(&s->h_run, sizeof(RunDev)) != cudaSuccess) {
+      cudaGetLastError();
+      s->h_run = nullptr;
+      pbg_set_error_message("cudaMallocHost of the run report failed");
+      return PBG_ERR_NOMEM;
+    }
+  }
+  RunDev* h = static_cast<RunDev*>(s->h_run);
+  *h = RunDev{};
+  h->pool = pool;
+  h->pool_len = pool_len;
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->d_run, h, sizeof(RunDev), cudaMemcpyHostToDevice, st));
+  int rc = PBG_OK;
+  for (int k = 0; k < n_steps; ++k) {
+    const long long j = j0 + k;
+    const int bDff = j % diff_freq == 0, bDnf = j % lub_freq == 0, chol = j % chol_freq == 0;
+    const long long key = bDff | (bDnf << 1) | (chol << 2) | ((long long)s->force_zero << 3) |
+                          ((long long)s->ff << 4) | ((long long)s->M << 5);
+    if (key != s->run_key || dt != s->run_key_dt) {
+      drop_run_graph(s);
+      s->run_key = key;
+      s->run_key_dt = dt;
+      s->run_key_repeats = 0;
+    }
+    ++s->run_key_repeats;
+    if (!s->run_exec && !s->run_refused && s->run_key_repeats >= 2 && (rc = capture_run_step(s, dt, bDff, bDnf, chol)))
+      break;
+    if (s->run_exec) {
+      PBG_CUDA_TRY(cudaGraphLaunch(s->run_exec, st));
+      PBG_CUDA_TRY(cudaStreamSynchronize(st));
+      pbg_count_launches(s->run_fixed_kernels + s->run_round_kernels * h->rounds);
+      pbg_count_host_calls(1);
+    } else {
+      if ((rc = enqueue_run_start(s, dt, bDff, bDnf, chol, st))) break;
+      do {  // the rounds driven from the host: the same kernels, the verdict read after each
+        if ((rc = enqueue_run_round(s, st, 0, 0))) break;
+        PBG_CUDA_TRY(cudaMemcpyAsync(h, s->d_run, sizeof(RunDev), cudaMemcpyDeviceToHost, st));
+        PBG_CUDA_TRY(cudaStreamSynchronize(st));
+      } while (h->more);
+      if (rc) break;
+      if ((rc = enqueue_run_tail(s, st))) break;
+      PBG_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    s->in_step = false;
+    if (h->status) {
+      PBG_CUDA_TRY(cudaMemcpyAsync(s->pos, s->pos_snap, pos_bytes, cudaMemcpyDeviceToDevice, st));
+      PBG_CUDA_TRY(cudaStreamSynchronize(st));
+      if (h->status == RUN_NOISE) {
+        pbg_set_error_message("pbg_run: the noise pool ran out in step %lld", j);
+        rc = PBG_ERR_NOISE;
+      } else {
+        pbg_set_error_message("maximal number of move attempts exceeded in step %lld", j);
+        rc = PBG_ERR_ATTEMPTS;
+      }
+      break;
+    }
+    // factorisation failures of this step, as step_end reports them
+    for (int q = 0; q < 4; ++q) s->hflags[q] = h->flags[q];
+    if (h->flags[1] < 0 || h->flags[2] < 0 || h->flags[3] < 0) {
+      pbg_set_error_message("a device-wide wait in the factorisation gave up");
+      rc = PBG_ERR_BARRIER;
+      break;
+    }
+    if (h->flags[1] || h->flags[2] || h->flags[3]) {
+      pbg_set_error_message("matrix not positive definite (cholesky info %d, inverse info %d/%d)", h->flags[1],
+                            h->flags[2], h->flags[3]);
+      rc = PBG_ERR_NOT_SPD;
+      break;
+    }
+    s->report.steps_done++;
+    s->report.draws_consumed = h->used;
+    s->report.last_attempts = h->attempts;
+    s->report.max_attempts = std::max(s->report.max_attempts, h->attempts);
+  }
+  s->in_step = false;
+  return rc;
+}
+
 // Steps j0 .. j0+n_steps-1 of BD.py:177 with the noise taken in order from
 // `pool`: the protocol of Box.propagate (box.py:150-250) with the pool in
 // place of RandomState.  A step that runs out of noise or of move attempts
@@ -759,6 +1054,9 @@ int run(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int 
     pbg_set_error_message("pbg_run inside a step");
     return s->report.status = PBG_ERR_STATE;
   }
+  if (n_steps > 0 && s->p.propagation_scheme == PBG_SCHEME_ERMAK && !s->lub && !s->divergence &&
+      device_accessible(pool))
+    return s->report.status = run_device(s, j0, n_steps, dt, diff_freq, lub_freq, chol_freq, pool, pool_len, st);
   const int n = s->n;
   const size_t pos_bytes = (size_t)s->N * 3 * sizeof(double);
   long long used = 0;

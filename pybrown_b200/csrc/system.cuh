@@ -29,8 +29,8 @@ struct pbg_system {
   double* radii = nullptr;     // N
   int* conn = nullptr;         // N x N bond matrix or null
   double* force = nullptr;     // ld (3N used)
-  bool force_zero = true;
-  bool b_holds_lower_D = false;  // this step's D build also wrote B's lower triangle (and padding)      // the external force is known to be zero (pbg_set_force from host or NULL)
+  bool force_zero = true;        // the external force is known to be zero (pbg_set_force from host or NULL)
+  bool b_holds_lower_D = false;  // this step's D build also wrote B's lower triangle (and padding)
   void* D = nullptr;           // ld x ld, prec
   void* B = nullptr;           // ld x ld, prec, lower factor
   void* D0 = nullptr;          // midpoint: step-start D
@@ -65,6 +65,20 @@ struct pbg_system {
   int build_Dff = 1, build_Dnf = 1, cholesky = 1;
   int attempts = 0;
   pbg_step_report report{};    // outcome of the last pbg_run
+  // Device-side steps of pbg_run (Ermak scheme, noise pool in device memory):
+  // one CUDA graph per step -- the step start, a conditional WHILE node over
+  // the move attempts, the wrap -- captured once a step repeats with the same
+  // flags, dt and force state.
+  void* d_run = nullptr;                 // the run's device state (noise cursor, attempts, status)
+  void* h_run = nullptr;                 // pinned copy: upload before a step, report after it
+  cudaGraphExec_t run_exec = nullptr;
+  cudaStream_t cap_stream = nullptr, cap_stream2 = nullptr;
+  long long run_key = -1;                // step flags and force state of run_exec
+  double run_key_dt = 0;
+  int run_key_repeats = 0;
+  bool run_refused = false;              // the driver refused the capture: host-driven steps
+  long long run_fixed_kernels = 0;       // kernels per replay besides the attempt rounds
+  long long run_round_kernels = 0;       // kernels per attempt round
 };
 
 namespace pbg {
@@ -82,6 +96,8 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
 int step_end(pbg_system* s, cudaStream_t st, double* pos_out = nullptr);
 int run(pbg_system* s, long long j0, int n_steps, double dt, int diff_freq, int lub_freq, int chol_freq,
         const double* pool, long long pool_len, cudaStream_t st);
+// Drops pbg_run's captured step graph (the system's buffers or interactions changed).
+void drop_run_graph(pbg_system* s);
 int system_get_matrix(pbg_system* s, int which, double* out, cudaStream_t st);
 int system_set_matrix(pbg_system* s, int which, const double* in, cudaStream_t st);
 int set_immobile(pbg_system* s, int M, const double* pos, const double* radii, const int* order,
