@@ -2038,11 +2038,7 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
   if (precision == PBG_PREC_MIXED_FP64_DIAG)
     return launch_df<float, false>((float*)A, n, ld, info, invdiag, ints, err, st, nullptr, 0, SPIN_LIMIT,
                                    (float*)X);
-  if (X) {
-    pbg_set_error_message("cholesky: X = inv(L) is formed with FP64 or FP64-diagonal factorisations only");
-    return PBG_ERR_ARG;
-  }
-  return launch_df<float, true>((float*)A, n, ld, info, invdiag, ints, err, st);
+  return launch_df<float, true>((float*)A, n, ld, info, invdiag, ints, err, st, nullptr, 0, SPIN_LIMIT, (float*)X);
 }
 
 
@@ -2324,7 +2320,7 @@ int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st) {
     return PBG_ERR_ARG;
   }
   // the factorisation forms X's off-diagonal tiles in the same launch
-  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED_FP64_DIAG, info, w.invdiag, w.scratch, st, w.X);
+  int rc = launch_cholesky_df(w.F, ld, ld, PBG_PREC_MIXED, info, w.invdiag, w.scratch, st, w.X);
   if (rc != PBG_OK) return rc;
   return launch_trtri_diag(w.invdiag, w.X, ld, PBG_PREC_MIXED, st);
 }

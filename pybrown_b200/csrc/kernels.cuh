@@ -128,9 +128,9 @@ size_t cholesky_work_bytes(int ld, int precision);
 int launch_cholesky_ws(void* A, int n, int ld, int precision, int* info, void* work, cudaStream_t st);
 // cholesky_df.cu
 size_t df_work_bytes(int ld);
-// X (FP64 or FP64-diagonal factorisations): the same launch also forms the
-// off-diagonal tiles of X = inv(L) (ld x ld, lower; launch_trtri_diag copies
-// the diagonal ones from invdiag).
+// X (or null): the same launch also forms the off-diagonal tiles of
+// X = inv(L) (ld x ld, lower; launch_trtri_diag copies the diagonal ones from
+// invdiag).
 int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* invdiag, void* work,
                        cudaStream_t st, void* X = nullptr);
 size_t spd_inverse_work_bytes(int ld);

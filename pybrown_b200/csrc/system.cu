@@ -339,7 +339,8 @@ int compute_Dff(pbg_system* s, cudaStream_t st, bool fill_B) {
 }
 
 // Mixed lubricated path: G = chol(J R J) and X = inv(G) on the tensor cores
-// (FP64 diagonal tiles, 3xTF32 trailing updates); then inv(R) = J X^T X J.
+// (FP32 chain, 3xTF32 updates on the tensor cores, X formed in the same launch);
+// then inv(R) = J X^T X J.
 static int factor_reversed_R(pbg_system* s, int* info, cudaStream_t st) {
   const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
   const long long total = (long long)s->ld * s->ld;
