@@ -462,7 +462,9 @@ def run_ours(args, torch, dist, rank, world):
     # exception type and message) instead of costing the whole line.
     sections = (("lubrication", args.no_lub, run_lub_section), ("batch", args.no_batch, run_batch_section),
                 ("serve", args.no_serve, run_serve_section),
-                ("serve_full_stream", args.no_serve or args.no_serve_full, run_serve_full_section))
+                ("serve_full_stream", args.no_serve or args.no_serve_full, run_serve_full_section),
+                ("serve_full_stream_smallest_work", args.no_serve or args.no_serve_full or args.no_serve_sjf,
+                 lambda a, t: run_serve_full_section(a, t, policy="smallest_work")))
     for key, skip, fn in sections:
         if world != 1 or skip:
             continue
@@ -598,24 +600,27 @@ def run_serve_section(args, torch):
     return summary
 
 
-def run_serve_full_section(args, torch):
+def run_serve_full_section(args, torch, policy="fifo"):
     """The full serving stream: Poisson 50 requests/s for 60 s, N log-uniform
     in [16, 2048], radii uniform in [10, 40], phi 0.05, steps uniform in
     [100, 5000], dt 1 ps, mixed precision, device noise; wall clock.  One B200
     cannot keep up with it (about 5e7 bead-steps/s offered), so the run is
     cut: admissions end when the stream ends and the loop stops a drain time
     later; the requests still waiting or running are reported as backlog,
-    latencies are those of the completed requests."""
+    latencies are those of the completed requests.  policy: the admission
+    order among arrived requests (FIFO, or least remaining work first)."""
     from pybrown_b200.batch import ReplicaBatch
     from pybrown_b200.serve import Server, make_stream
     duration = 60.0
     stream = make_stream(4, rate=50.0, duration=duration, steps_min=100, steps_max=5000, dt=1.0, lazy=True)
-    server = Server(ReplicaBatch(precision="mixed"), keep_positions=False, max_active=args.serve_max_active)
+    server = Server(ReplicaBatch(precision="mixed"), keep_positions=False, max_active=args.serve_max_active,
+                    policy=policy)
     recs, summary = server.run(stream, clock="wall", stop_admission_at=duration, drain_limit=args.serve_drain)
     server.batch.close()
     summary["workload"] = ("Poisson 50 req/s for 60 s, N log-U[16,2048], a~U[10,40], phi=0.05, steps U[100,5000], "
                            "dt=1, mixed, device noise; admissions end at 60 s, the loop "
-                           f"{args.serve_drain:g} s later; at most {args.serve_max_active} requests run together")
+                           f"{args.serve_drain:g} s later; at most {args.serve_max_active} requests run together; "
+                           f"admission {policy}")
     summary["offered_bead_steps_per_s"] = sum(r.n_beads * r.steps for r in stream) / duration
     summary["completed_bead_steps"] = sum(r.n_beads * r.steps for r in recs if math.isfinite(r.completed))
     summary["memory_budget_gb"] = summary.pop("memory_budget") / 1e9
@@ -656,6 +661,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving stream")
     ap.add_argument("--serve-steps", type=int, nargs=2, default=(5, 30), help="steps per request: min max")
     ap.add_argument("--no-serve-full", action="store_true", help="skip the full 60 s serving stream")
+    ap.add_argument("--no-serve-sjf", action="store_true",
+                    help="skip the full stream under the least-remaining-work admission policy")
     ap.add_argument("--serve-drain", type=float, default=60.0,
                     help="full serving stream: seconds the loop runs on after admissions end")
     ap.add_argument("--serve-max-active", type=int, default=256,

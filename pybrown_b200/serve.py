@@ -24,6 +24,7 @@ reaches them) and ``"virtual"`` (time advances by ``tick`` per batched step
 and jumps to the next arrival when idle; deterministic, for tests).
 """
 import collections
+import heapq
 import math
 import time
 from dataclasses import dataclass, field
@@ -172,9 +173,19 @@ class Server:
     batch: a ReplicaBatch (or an object with add/remove/propagate/positions/
     footprint); memory_budget: device bytes the admitted requests may take
     (default: 80 % of the free device memory at start); max_active: optional
-    cap on concurrent requests."""
+    cap on concurrent requests; policy: the admission order among the
+    requests that have arrived -- "fifo" (arrival order; a request that does
+    not fit holds back the ones behind it) or "smallest_work" (least
+    remaining work first, work = steps x (3N)^3, the factorisation's cost per
+    step, ties in arrival order)."""
 
-    def __init__(self, batch=None, memory_budget=None, max_active=None, precision="mixed", keep_positions=True):
+    POLICIES = ("fifo", "smallest_work")
+
+    def __init__(self, batch=None, memory_budget=None, max_active=None, precision="mixed", keep_positions=True,
+                 policy="fifo"):
+        if policy not in self.POLICIES:
+            raise ValueError(f"unknown admission policy {policy!r}")
+        self.policy = policy
         if batch is None:
             from .batch import ReplicaBatch
             batch = ReplicaBatch(precision=precision)
@@ -219,6 +230,7 @@ class Server:
             if self.batch.footprint(r.n_beads) > self.memory_budget:
                 raise ValueError(f"request {r.rid} (N={r.n_beads}) does not fit in the memory budget")
         pending = collections.deque(reqs)
+        arrived = []  # smallest_work: heap of the arrived requests
         records = {r.rid: Record(r.rid, r.n_beads, r.steps, r.arrival) for r in reqs}
         active = {}  # slot -> [request, steps left, bytes]
         used = 0
@@ -233,20 +245,36 @@ class Server:
         def now():
             return vnow if clock == "virtual" else time.perf_counter() - start
 
-        while pending or active:
+        def next_candidate():
+            if self.policy == "fifo":
+                return pending[0] if pending and pending[0].arrival <= t else None
+            while pending and pending[0].arrival <= t:
+                r = pending.popleft()
+                heapq.heappush(arrived, (r.steps * (3 * r.n_beads) ** 3, r.arrival, r.rid, r))
+            return arrived[0][3] if arrived else None
+
+        def take(r):
+            if self.policy == "fifo":
+                pending.popleft()
+            else:
+                heapq.heappop(arrived)
+
+        while pending or arrived or active:
             t = now()
             if end_at is not None and t >= end_at:
                 break
             admitting = stop_admission_at is None or t < stop_admission_at
             if not admitting and not active:
                 break
-            # admission: arrived requests, in arrival order, while they fit
-            while admitting and pending and pending[0].arrival <= t:
-                r = pending[0]
+            # admission: arrived requests in policy order, while they fit
+            while admitting:
+                r = next_candidate()
+                if r is None:
+                    break
                 fp = self.batch.footprint(r.n_beads)
                 if used + fp > self.memory_budget or (self.max_active and len(active) >= self.max_active):
                     break
-                pending.popleft()
+                take(r)
                 t0 = time.perf_counter()
                 slot = self.batch.add(r.materialize(), r.radii, r.box_length, T=r.T, viscosity=r.viscosity,
                                       seed=r.seed, noise="device")
@@ -257,6 +285,8 @@ class Server:
             peak_used = max(peak_used, used)
             peak_active = max(peak_active, len(active))
             if not active:
+                if not pending:
+                    break  # admission closed with requests still waiting
                 # idle until the next arrival
                 nxt = pending[0].arrival
                 if stop_admission_at is not None and nxt >= stop_admission_at:

@@ -175,3 +175,24 @@ def test_failed_factorisation_drops_only_that_request():
     assert recs[1].failed == {"status": 7, "recheck": 0} and math.isnan(recs[1].completed)
     assert b.steps[0] == 6 and b.steps[2] == 6
     assert summary["failures"][0]["rid"] == 1
+
+
+def test_smallest_work_policy_admits_the_cheapest_first():
+    """With one request at a time, FIFO admits in arrival order and
+    smallest_work in order of steps x (3N)^3 (ties by arrival)."""
+    reqs = [_req(0, 0.0, 40, 4), _req(1, 0.0, 10, 6), _req(2, 0.0, 20, 2), _req(3, 0.0, 10, 6)]
+    order = {}
+    for policy in ("fifo", "smallest_work"):
+        b = FakeBatch()
+        server = Server(b, memory_budget=10 ** 9, max_active=1, policy=policy)
+        recs, summary = server.run(reqs, clock="virtual", tick=1e-3)
+        assert summary["completed"] == 4
+        order[policy] = [r.rid for r in sorted(recs, key=lambda x: x.admitted)]
+    assert order["fifo"] == [0, 1, 2, 3]
+    # work: rid 2: 2 * 60^3 = 432000, rids 1 and 3: 6 * 30^3 = 162000, rid 0: 4 * 120^3
+    assert order["smallest_work"] == [1, 3, 2, 0]
+
+
+def test_unknown_policy_is_rejected():
+    with pytest.raises(ValueError):
+        Server(FakeBatch(), memory_budget=1, policy="random")
