@@ -27,10 +27,13 @@ def _serve(reqs, **kw):
     return {r.rid: r for r in recs}, summary
 
 
-def test_result_is_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("policy", ["fifo", "smallest_work"])
+def test_result_is_the_same_alone_and_in_the_mix(policy):
+    """Under either admission policy (which only changes when a request runs
+    and with whom)."""
     stream = [_request(0, 0.000, 60, 9, 11), _request(1, 0.002, 150, 4, 12), _request(2, 0.0035, 25, 12, 13),
               _request(3, 0.006, 90, 6, 14), _request(4, 0.0, 33, 2, 15)]
-    mixed, summary = _serve(stream)
+    mixed, summary = _serve(stream, policy=policy)
     assert summary["peak_active"] >= 3
     for r in stream:
         alone, _ = _serve([Request(r.rid, 0.0, r.positions, r.radii, r.box_length, r.steps, r.seed)])
