@@ -80,16 +80,13 @@ __global__ void reverse_narrow_kernel(const double* __restrict__ R, int ld, floa
     F[t] = (float)R[total - 1 - t];
 }
 
-// res = b - R x in FP64 (one warp per row, fixed shuffle tree).
+// res = b - R x in FP64 (one warp per row: 16-byte loads, four in flight per
+// lane, fixed shuffle tree; row_dot).
 __global__ void residual_kernel(const double* __restrict__ R, int ld, int n, const double* __restrict__ b,
                                 const double* __restrict__ x, double* __restrict__ res) {
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (row >= n) return;
-  const double* r = R + (size_t)row * ld;
-  double s = 0.0;
-  for (int j = lane; j < n; j += 32) s += r[j] * x[j];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const double s = row_dot(R + (size_t)row * ld, n, [&](int j, double r) { return r * x[j]; });
   if (lane == 0) res[row] = b[row] - s;
 }
 
