@@ -24,7 +24,6 @@ namespace pbg {
 namespace tc {
 
 constexpr int TILE = 64;
-constexpr uint32_t KBLOCK_BYTES_PER_ROW = 128;  // 32 FP32 per swizzled row
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -133,38 +132,6 @@ __device__ __forceinline__ uint32_t sw128_offset(int R, int r, int c) {
 // Bytes of the hi and lo halves of an R-row operand.
 __host__ __device__ constexpr uint32_t operand_bytes(int R) { return (uint32_t)R * TILE * 4; }
 
-// Loads `nt` 64 x 64 FP32 tiles (tiles[q], row stride ld; L2 loads) and
-// writes their hi / lo TF32 halves as rows q * 64 .. q * 64 + 63 of the
-// R-row operands at hi and lo.  All CTA threads (nthreads) call it; each thread
-// keeps its loads of one tile in flight before converting.
-template <int NTHREADS>
-__device__ __forceinline__ void split_tiles(const float* const* tiles, int nt, int ld, int R, unsigned char* hi,
-                                            unsigned char* lo) {
-  constexpr int PER = TILE * 16 / NTHREADS;  // 16-byte chunks per thread per tile
-  for (int q = 0; q < nt; ++q) {
-    float4 v[PER];
-#pragma unroll
-    for (int e = 0; e < PER; ++e) {
-      const int t = threadIdx.x + e * NTHREADS, r = t >> 4, c = t & 15;
-      v[e] = __ldcg(reinterpret_cast<const float4*>(tiles[q] + (size_t)r * ld + 4 * c));
-    }
-#pragma unroll
-    for (int e = 0; e < PER; ++e) {
-      const int t = threadIdx.x + e * NTHREADS, r = q * TILE + (t >> 4), c = t & 15;
-      const uint32_t off = sw128_offset(R, r, c);
-      const float x[4] = {v[e].x, v[e].y, v[e].z, v[e].w};
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        h[u] = rna_tf32(x[u]);
-        l[u] = rna_tf32(x[u] - __uint_as_float(h[u]));
-      }
-      *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-    }
-  }
-}
-
 // One 64 x 64 FP32 source tile and where its TF32 halves go: rows
 // row0 .. row0 + 63 of the R-row operands at hi and lo.
 struct SplitTile {
@@ -174,9 +141,10 @@ struct SplitTile {
   unsigned char* lo;
 };
 
-// split_tiles for up to MAXT tiles at once: every thread issues all of its
-// loads (16 bytes each, L2) before the first conversion, so the tiles cost
-// one memory round trip together.
+// Loads up to MAXT 64 x 64 FP32 tiles (row stride ld) and writes their hi /
+// lo TF32 halves into the operands: every thread issues all of its loads
+// (16 bytes each, through L2) before the first conversion, so the tiles cost
+// one memory round trip together.  All NTHREADS threads of the CTA call it.
 template <int NTHREADS, int MAXT>
 __device__ __forceinline__ void split_tiles_all(const SplitTile (&t)[MAXT], int count, int ld) {
   constexpr int PER = TILE * 16 / NTHREADS;
