@@ -6,6 +6,8 @@
 // four in flight per lane (row_dot), FP64 accumulation, fixed shuffle tree
 // (so a result does not depend on scheduling).  B is lower triangular and
 // only its lower part is read.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "propagate.cuh"
@@ -112,6 +114,96 @@ __global__ void __launch_bounds__(256) trsv_upper_step_kernel(const T* __restric
   }
 }
 
+__device__ __forceinline__ int trsv_ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void trsv_st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr long long TRSV_SPIN_LIMIT = 1LL << 24;
+
+// The whole back substitution B^T y = rhs in one launch: CTA K owns block row
+// K of the upper system.  For I = nt-1 down to K+1 (the fixed order of the
+// per-step launches) it waits for y_I to be published, then accumulates
+// B_IK^T y_I; the tile B_IK for the next I is already in registers while it
+// waits.  Thread (c, g) (c = tid % 64, g = tid / 64) sums rows 16g .. 16g+15
+// of column c; the four partial sums meet in a fixed order, so the result
+// does not depend on scheduling.  Then y_K = inv(B_KK)^T r_K from the
+// inverted diagonal tile (staged in shared memory at the start, before any
+// wait), stored, and flags[K] released.  All CTAs are co-resident (cooperative
+// launch).  A wait that gives up after spin_limit polls sets *err = -1 and
+// the CTA still publishes (y_K then NaN), so no other CTA waits on it.
+template <typename T>
+__global__ void __launch_bounds__(256) trsv_upper_df_kernel(const T* __restrict__ B, int ld, int nt,
+                                                            const T* __restrict__ invdiag,
+                                                            const double* __restrict__ rhs, double* y,
+                                                            int* flags, int* err, long long spin_limit) {
+  constexpr int nb = PBG_TILE, G = 4, R = nb / G;
+  __shared__ T s_d[nb * nb];
+  __shared__ double s_part[G][nb];
+  __shared__ double s_r[nb];
+  __shared__ int s_ok;
+  const int tid = threadIdx.x, c = tid % nb, g = tid / nb;
+  const int K = nt - 1 - (int)blockIdx.x;  // the first CTAs scheduled start the chain
+  const T* D = invdiag + (size_t)K * nb * nb;
+  for (int e = tid; e < nb * nb; e += blockDim.x) s_d[e] = D[e];
+  const double r0 = tid < nb ? rhs[(size_t)K * nb + tid] : 0.0;
+  if (tid == 0) s_ok = 1;
+  // column c of B_IK, rows 16g .. 16g+15
+  auto load_tile = [&](int I, T (&v)[R]) {
+    const T* b = B + ((size_t)I * nb + g * R) * ld + (size_t)K * nb + c;
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = b[(size_t)j * ld];
+  };
+  T nxt[R];
+  double acc = 0.0;
+  if (nt - 1 > K) load_tile(nt - 1, nxt);
+  for (int I = nt - 1; I > K; --I) {
+    T cur[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) cur[j] = nxt[j];
+    if (I - 1 > K) load_tile(I - 1, nxt);
+    if (tid == 0) {
+      long long it = 0;
+      while (trsv_ld_acquire(flags + I) == 0)
+        if (++it > spin_limit) {
+          atomicExch(err, -1);
+          s_ok = 0;
+          break;
+        }
+    }
+    __syncthreads();
+    double yv[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) yv[j] = __ldcg(y + (size_t)I * nb + g * R + j);
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc += (double)cur[j] * yv[j];
+  }
+  s_part[g][c] = acc;
+  __syncthreads();
+  if (tid < nb) s_r[tid] = r0 - ((s_part[0][tid] + s_part[1][tid]) + (s_part[2][tid] + s_part[3][tid]));
+  __syncthreads();
+  // y_K[c] = sum_{k >= c} invL[k][c] r_K[k]
+  double q = 0.0;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const int k = g * R + j;
+    if (k >= c) q += (double)s_d[k * nb + c] * s_r[k];
+  }
+  s_part[g][c] = q;
+  __syncthreads();
+  if (tid < nb) {
+    const double v = (s_part[0][tid] + s_part[1][tid]) + (s_part[2][tid] + s_part[3][tid]);
+    y[(size_t)K * nb + tid] = s_ok ? v : __longlong_as_double(0x7ff8000000000000LL);
+    __threadfence();
+  }
+  __syncthreads();
+  if (tid == 0) trsv_st_release(flags + K, 1);
+}
+
 inline int rows_grid(int n) { return (n * 32 + 255) / 256; }
 inline int vec_grid(int n) { return (n + 255) / 256; }
 
@@ -173,9 +265,55 @@ int launch_drift_combine(const double* Dy, const double* Bxi, const double* ddet
   return PBG_OK;
 }
 
-int launch_trsv_upper(const void* B, int ld, int precision, const void* invdiag, const double* rhs,
-                      double* r_work, double* y, cudaStream_t st) {
+namespace {
+
+// CTAs of trsv_upper_df_kernel<T> that fit on the current device at once.
+template <typename T>
+int trsv_df_capacity() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (!cached[dev]) {
+    int bps = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trsv_upper_df_kernel<T>, 256, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 0;
+    cached[dev] = std::max(1, bps * sms);
+  }
+  return cached[dev];
+}
+
+template <typename T>
+int launch_trsv_df(const T* B, int ld, const T* invdiag, const double* rhs, double* y, int* flags, int* err,
+                   cudaStream_t st) {
   const int nt = ld / PBG_TILE;
+  PBG_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)nt * sizeof(int), st));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nt);
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, trsv_upper_df_kernel<T>, B, ld, nt, invdiag, rhs, y, flags, err,
+                                  TRSV_SPIN_LIMIT));
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
+}
+
+}  // namespace
+
+int launch_trsv_upper(const void* B, int ld, int precision, const void* invdiag, const double* rhs,
+                      double* r_work, double* y, int* flags, int* err, cudaStream_t st) {
+  const int nt = ld / PBG_TILE;
+  if (flags && err) {
+    if (precision == PBG_PREC_FP64 && nt <= trsv_df_capacity<double>())
+      return launch_trsv_df((const double*)B, ld, (const double*)invdiag, rhs, y, flags, err, st);
+    if (precision != PBG_PREC_FP64 && nt <= trsv_df_capacity<float>())
+      return launch_trsv_df((const float*)B, ld, (const float*)invdiag, rhs, y, flags, err, st);
+  }
   PBG_CUDA_TRY(cudaMemcpyAsync(r_work, rhs, (size_t)ld * sizeof(double), cudaMemcpyDeviceToDevice, st));
   for (int I = nt - 1; I >= 0; --I) {
     const int grid = I > 0 ? I : 1;

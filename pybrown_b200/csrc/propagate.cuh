@@ -72,7 +72,10 @@ int launch_drift_combine(const double* Dy, const double* Bxi, const double* ddet
                          double* drift, cudaStream_t st);
 // Solves B^T y = rhs (B lower, order ld, padded); invdiag are the inverted
 // diagonal tiles left by the Cholesky workspace; rhs, r_work, y have ld entries.
+// With flags (ld / 64 ints of scratch) and err, one cooperative data-flow
+// launch when its ld / 64 CTAs fit on the device (a wait that gives up sets
+// *err = -1); otherwise, or with null flags, one launch per block row.
 int launch_trsv_upper(const void* B, int ld, int precision, const void* invdiag, const double* rhs,
-                      double* r_work, double* y, cudaStream_t st);
+                      double* r_work, double* y, int* flags, int* err, cudaStream_t st);
 
 }  // namespace pbg

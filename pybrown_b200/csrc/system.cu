@@ -139,7 +139,7 @@ void destroy_system(pbg_system* s) {
                   s->Mff,  s->Rff,      s->R,     s->Mff0,  s->Rff0,  s->R0,    s->FX,   s->U,
                   s->BX,   s->ddet,     s->y,     s->rwork, s->Dy,    s->drift, s->xi,   s->phase,
                   s->chol_work, s->inv_work, s->dflags, s->div, s->sol, s->sol0, s->res, s->corr,
-                  s->G};
+                  s->G,    s->tflags};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->hflags) cudaFreeHost(s->hflags);
@@ -210,6 +210,7 @@ int create_system(const pbg_params* prm, pbg_system** out) {
   if (s->smith) SYS_ALLOC(s->phase, phase_scratch_bytes(s->N, s->tables, s->prec));
   SYS_ALLOC(s->chol_work, cholesky_work_bytes(s->ld, s->prec));
   SYS_ALLOC(s->dflags, 8 * sizeof(int));
+  SYS_ALLOC(s->tflags, (ld / PBG_TILE) * sizeof(int));
   if (cudaMallocHost((void**)&s->hflags, 8 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     destroy_system(s);
@@ -681,7 +682,8 @@ int step_attempt(pbg_system* s, const double* xi, int* accepted, cudaStream_t st
   // stochastic drift m/2 sqrt(2 dt) (D' inv(B0^T) - B0) @ xi = c2 (D' y - B0 xi), B0^T y = xi
   if (s->mlub && s->g_valid) {
     if ((rc = midpoint_y_from_G(s, st))) return rc;
-  } else if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, st))) {
+  } else if ((rc = launch_trsv_upper(s->B, s->ld, s->prec, s->chol_work, s->xi, s->rwork, s->y, s->tflags,
+                                       s->dflags + 4, st))) {
     return rc;
   }
   if (s->mlub) {
@@ -732,9 +734,14 @@ int step_end(pbg_system* s, cudaStream_t st, double* pos_out) {
   }
   if (pos_out) PBG_CUDA_TRY(cudaMemcpyAsync(s->hpos, s->pos, pos_bytes, cudaMemcpyDeviceToHost, st));
   // surface factorisation failures of this step
-  PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  PBG_CUDA_TRY(cudaMemcpyAsync(s->hflags, s->dflags, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
   PBG_CUDA_TRY(cudaStreamSynchronize(st));
   if (pos_out) std::memcpy(pos_out, s->hpos, pos_bytes);
+  if (s->hflags[4] < 0) {
+    PBG_CUDA_TRY(cudaMemsetAsync(s->dflags + 4, 0, sizeof(int), st));
+    pbg_set_error_message("a device-wide wait in the back substitution gave up");
+    return PBG_ERR_BARRIER;
+  }
   if (s->hflags[1] < 0 || s->hflags[2] < 0 || s->hflags[3] < 0) {
     pbg_set_error_message("a device-wide wait in the factorisation gave up");
     return PBG_ERR_BARRIER;

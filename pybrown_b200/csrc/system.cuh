@@ -42,7 +42,9 @@ struct pbg_system {
   void* phase = nullptr;       // Ewald phase tables
   void* chol_work = nullptr;   // inverted diagonal tiles of B
   void* inv_work = nullptr;    // SPD inverse workspace (tensor-core inverse workspace if mlub)
-  int* dflags = nullptr;       // [0] overlap, [1] cholesky info, [2] Rff info, [3] D info
+  int* dflags = nullptr;       // [0] overlap, [1] cholesky info, [2] Rff info, [3] D info,
+                               // [4] back-substitution wait (-1: gave up)
+  int* tflags = nullptr;       // ld / 64 block-row flags of the one-launch back substitution
   bool divergence = false;     // divergence term of the lubricated D (Ermak scheme)
   double* div = nullptr;       // ld: its value this step
   int* hflags = nullptr;       // pinned mirror
