@@ -783,7 +783,7 @@ PBG_API int pbg_batch_add(pbg_batch* b, const pbg_params* p, const double* pos, 
   const size_t ph = phase_scratch_bytes(r->N, b->tables, b->precision);
   if (ok && ph) ok = pool_alloc(&r->phase, ph);
   std::vector<int4> tasks;
-  cholesky_replica_tasks(r->nt, tasks, r->seg_start);
+  cholesky_replica_tasks(r->nt, b->precision, tasks, r->seg_start);
   if (ok && !tasks.empty()) {
     ok = pool_alloc(&r->tasks, tasks.size() * sizeof(int4)) &&
          cudaMemcpyAsync(r->tasks, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, 0) ==
@@ -1341,7 +1341,12 @@ PBG_API int pbg_batch_autotune(pbg_batch* b, int reps, int* best, float* ms, voi
   cudaStream_t st = (cudaStream_t)stream;
   const int R = (int)b->active.size();
   const bool f64 = b->precision == PBG_PREC_FP64;
-  const int max_ctas = f64 ? 1 : 2;
+  int max_ctas = 1, sms = 0;
+  if (R) {
+    const int rr = cholesky_batch_residency(b->precision, &max_ctas, &sms);
+    if (rr) return rr;
+  }
+  max_ctas = std::min(max_ctas, 2);
   if (ms)
     for (int c = 0; c < 2 * PBG_MERGE_ORDERS; ++c) ms[c] = -1.0f;
   const int old_order = b->merge_order, old_ctas = b->ctas_per_sm;

@@ -103,6 +103,12 @@ __device__ __forceinline__ int smid() {
 }
 #define TRACE(slot, t) \
   if (threadIdx.x == 0 && (t) < 65536) g_task_trace[4 * (t) + (slot)] = (slot) == 3 ? smid() : gtimer()
+// Phase totals of the left-looking batch workers: per CTA, 16 slots of
+// clock64 cycles or counts (see ll_task).
+__device__ long long g_ll_prof[1024 * 16];
+#define LLPROF(slot, v) \
+  if (threadIdx.x == 0 && blockIdx.x < 1024) g_ll_prof[blockIdx.x * 16 + (slot)] += (v)
+#define LLCLK() clock64()
 // Finer timeline of the FP32 chain: 8 stamps per panel k.
 __device__ long long g_chain_trace[8 * 1024];
 #define CTRACE(k, slot) \
@@ -110,6 +116,8 @@ __device__ long long g_chain_trace[8 * 1024];
 #else
 #define TRACE(slot, t)
 #define CTRACE(k, slot)
+#define LLPROF(slot, v) ((void)(v))
+#define LLCLK() 0LL
 #endif
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
@@ -1780,6 +1788,415 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_ke
   batch_worker_loop<T>(reps, tasks, ntasks, ctl, smem);
 }
 
+// ---------------------------------------------------------------- left-looking batched factorisation
+// The mixed batch factors every replica left-looking on the tcgen05 tensor
+// cores.  A task owns the row tiles i and i + 1 of column j of L (only i
+// when i + 1 = nt) and forms
+//   U_rj = A_rj - sum_{k < j} L_rk L_jk^T        (r = i, i + 1)
+// as one M = 128, N = 64, K = 64 j product accumulated in TMEM: for each k
+// the tiles L_ik, L_{i+1,k}, L_jk are split into TF32 hi / lo halves in
+// shared memory and three MMAs per K-step add A_hi B_hi + A_hi B_lo + A_lo
+// B_hi to the accumulator, while the tiles of k + 1 and k + 2 are on their
+// way (cp.async into two raw FP32 stages).  Then, by the task's kind:
+//   LL_DIAG (i = j): F(j) -- L_jj and inv(L_jj) in FP32, as the FP32 chain
+//     forms them -- published at once, then S(j + 1, j) = U inv(L_jj)^T with
+//     the inverse still in shared memory;
+//   LL_UPDATE (i > j): U written over A's tiles, upd[r] = j + 1;
+//   LL_SOLVE (i > j, a later segment): S(i, j), S(i + 1, j) from the stored
+//     U once F(j) is published.
+// Every tile is read as A once and written twice (U, then L), where a
+// right-looking update reads and writes its tile once per panel.  Flags:
+// fin[r] = the number of final tiles of row r, upd[r] = the columns of row r
+// whose U is stored.  A row's tiles become final in column order (tile
+// (r, j) needs (r, j - 1)), so one counter per row says which L_rk are
+// ready.  Every task depends only on earlier tasks of the list.
+constexpr uint32_t LL_A_BYTES = tc::operand_bytes(128);
+constexpr uint32_t LL_B_BYTES = tc::operand_bytes(64);
+constexpr uint32_t LL_OPERAND_BYTES = 2 * LL_A_BYTES + 2 * LL_B_BYTES;
+// The operands (from the 1024-byte aligned start of dynamic shared memory),
+// two raw FP32 stages of a K-step's tiles, then the worker's words
+// (LLShared).  After the last product the operand bytes hold P ([128][LDA]
+// floats from 0), the U tiles ([64][LDA] at LL_U0 and LL_U1) and the factor
+// scratch (from 0).
+struct LLShared {
+  uint64_t mbar;
+  uint32_t tmem;
+  int task, ok, seen[3];
+};
+constexpr uint32_t LL_RAW_BYTES = 3 * NB * NB * sizeof(float);  // one raw stage: L_ik, L_{i+1,k}, L_jk
+constexpr uint32_t LL_SHARED_OFFSET = LL_OPERAND_BYTES + 2 * LL_RAW_BYTES;
+constexpr size_t ll_smem_bytes() { return LL_SHARED_OFFSET + sizeof(LLShared); }
+static_assert(ll_smem_bytes() <= 227 * 1024, "the worker does not fit an SM");
+// task kinds of the left-looking list
+enum : int { LL_DIAG = 0, LL_UPDATE = 1, LL_SOLVE = 2 };
+constexpr uint32_t LL_U0 = 40960, LL_U1 = 61440;
+static_assert(factor_task_f32_smem_bytes() <= LL_U0, "the factor scratch overlaps U0");
+static_assert(sizeof(float) * 128 * LDA <= LL_U0, "P overlaps U0");
+static_assert(LL_U1 + sizeof(float) * NB * LDA <= LL_OPERAND_BYTES, "U1 lies outside the operand bytes");
+
+struct LLWorker {
+  uint64_t* mbar;       // completion of the products of one K-step
+  uint32_t tmem;        // TMEM base: the 128 x 64 FP32 accumulator
+  uint32_t phase;
+  unsigned char* base;  // 1024-byte aligned operand area
+};
+
+__device__ __forceinline__ DFArgs batch_args(const CholRep& R, const int4* tasks, int ntasks, int* ctl) {
+  DFArgs a;
+  a.A = R.A;
+  a.ld = R.ld;
+  a.n = R.n;
+  a.nt = R.nt;
+  a.ntasks = ntasks;
+  a.tasks = tasks;
+  a.ctl = ctl;
+  a.upd = R.upd;
+  a.fin = R.fin;
+  a.info = R.info;
+  a.invdiag = R.invdiag;
+  a.err = reinterpret_cast<unsigned*>(ctl + 3);
+  a.spin_limit = SPIN_LIMIT;
+  a.X = nullptr;
+  a.xupd = nullptr;
+  a.xfin = nullptr;
+  return a;
+}
+
+// Warp 0 waits until base[rows[q]] >= target for every slot q in mask
+// (bounded, with the abort polling of wait_all).  seen[q] (touched by warp 0
+// only) keeps the largest count observed for slot q in this task, so a wait
+// that an earlier observation already satisfies costs no memory round trip.
+// *s_ok only ever goes from 1 to 0.  Ends with a CTA barrier.
+__device__ bool ll_wait_rows(const DFArgs& a, const int* base, const int (&rows)[3], unsigned mask, int target,
+                             int* seen, int* s_ok) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const bool mine = lane < 3 && ((mask >> lane) & 1u);
+    const int* flag = mine ? base + rows[lane < 3 ? lane : 0] : nullptr;
+    bool done = !mine || seen[lane] >= target;
+    bool ok = true;
+    for (long long it = 0;; ++it) {
+      if (!done) {
+        const int v = ld_acquire(flag);
+        if (v >= target) {
+          seen[lane] = v;
+          done = true;
+        }
+      }
+      if (__all_sync(0xffffffffu, done)) break;
+      if ((it & 15) == 15) {
+        const int ab = __shfl_sync(0xffffffffu, lane == 0 ? ld_acquire(a.ctl + 1) : 0, 0);
+        if (ab) {
+          ok = false;
+          break;
+        }
+      }
+      if (it + 1 > a.spin_limit) {
+        if (lane == 0) {
+          atomicExch(a.ctl + 1, 1);
+          atomicAdd(a.ctl + 2, 1);
+          atomicOr(a.err, PBG_DEV_ERR_BARRIER);
+          atomicCAS(a.info, 0, -1);
+        }
+        ok = false;
+        break;
+      }
+      if (it > 256) __nanosleep(200);
+    }
+    if (lane == 0 && !ok) *s_ok = 0;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// Waits (bounded) for the products of the last commit; one verdict for the
+// CTA.  A failure aborts the run like an expired flag wait.
+__device__ bool ll_mma_wait(const DFArgs& a, LLWorker& w) {
+  bool ok = tc::mbar_wait(w.mbar, w.phase, a.spin_limit);
+  if (!ok) ok = tc::mbar_wait(w.mbar, w.phase, a.spin_limit);  // the MMAs must not outlive the TMEM
+  ok = __syncthreads_and(ok) != 0;
+  w.phase ^= 1;
+  if (!ok && threadIdx.x == 0) {
+    atomicExch(a.ctl + 1, 1);
+    atomicOr(a.err, PBG_DEV_ERR_BARRIER);
+    atomicCAS(a.info, 0, -1);
+  }
+  tc::fence_after_sync();
+  return ok;
+}
+
+// cp.async (16 bytes, through L2) of this thread's share of a 64 x 64 FP32
+// tile into a row-major [64][64] stage; the same thread converts the same
+// chunks later, so its own wait_group makes them visible to it.
+__device__ __forceinline__ void ll_fetch_tile(const float* src, int ld, float* raw) {
+#pragma unroll
+  for (int e = 0; e < tc::TileShare<THREADS>::PER; ++e) {
+    const int q = threadIdx.x + e * THREADS, r = q >> 4, c = q & 15;
+    cp_async16(raw + r * NB + 4 * c, src + (size_t)r * ld + 4 * c);
+  }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The tiles of K-step k (L_ik, L_{i+1,k}, L_jk) into a raw stage, one group.
+__device__ __forceinline__ void ll_fetch_step(const DFArgs& a, int i, bool two, int j, int k, float* raw) {
+  ll_fetch_tile(tile<float>(a, i, k), a.ld, raw);
+  if (two) ll_fetch_tile(tile<float>(a, i + 1, k), a.ld, raw + NB * NB);
+  ll_fetch_tile(tile<float>(a, j, k), a.ld, raw + 2 * NB * NB);
+  cp_async_commit();
+}
+
+// This thread's share of a raw stage tile, back into registers.
+__device__ __forceinline__ void ll_share_from_raw(const float* raw, tc::TileShare<THREADS>& s) {
+#pragma unroll
+  for (int e = 0; e < tc::TileShare<THREADS>::PER; ++e) {
+    const int q = threadIdx.x + e * THREADS, r = q >> 4, c = q & 15;
+    s.v[e] = *reinterpret_cast<const float4*>(raw + r * NB + 4 * c);
+  }
+}
+
+// P = sum_{k < j} [L_ik; L_{i+1,k}] L_jk^T into shared memory ([128][LDA]
+// floats at the operand area's start), for j > 0.  The tiles of K-step k + 2
+// are fetched (cp.async, two raw stages) while the products of k run and
+// the tiles of k + 1 wait converted-to-be; the rows' counters are waited for
+// before each fetch.  Returns false if the run was aborted (nothing of this
+// CTA in flight then).
+__device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* seen, int* s_ok) {
+  const int tid = threadIdx.x;
+  const bool two = i + 1 < a.nt;
+  unsigned char* Ahi = w.base;
+  unsigned char* Alo = Ahi + LL_A_BYTES;
+  unsigned char* Bhi = Alo + LL_A_BYTES;
+  unsigned char* Blo = Bhi + LL_B_BYTES;
+  float* raw[2] = {reinterpret_cast<float*>(w.base + LL_OPERAND_BYTES),
+                   reinterpret_cast<float*>(w.base + LL_OPERAND_BYTES + LL_RAW_BYTES)};
+  const int rows[3] = {i, two ? i + 1 : i, j};
+  if (!two) {
+    // rows 64 .. 127 of both A halves stay zero for the whole task: bytes
+    // 8192 .. 16383 of each of the two K blocks (16384 bytes each)
+    for (int e = tid; e < 4 * 512; e += THREADS) {
+      const int part = e >> 9, off = (e & 511) * 16;
+      unsigned char* p = (part & 1 ? Alo : Ahi) + (part >> 1) * 16384 + 8192 + off;
+      *reinterpret_cast<uint4*>(p) = make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+  long long c0 = LLCLK();
+  if (!ll_wait_rows(a, a.fin, rows, 7u, 1, seen, s_ok)) return false;
+  ll_fetch_step(a, i, two, j, 0, raw[0]);
+  if (j > 1) {
+    if (!ll_wait_rows(a, a.fin, rows, 7u, 2, seen, s_ok)) {
+      cp_async_wait_group<0>();
+      return false;
+    }
+    ll_fetch_step(a, i, two, j, 1, raw[1]);
+  }
+  LLPROF(2, LLCLK() - c0);
+  for (int k = 0; k < j; ++k) {
+    float* st = raw[k & 1];
+    c0 = LLCLK();
+    if (k + 1 < j) cp_async_wait_group<1>();
+    else cp_async_wait_group<0>();
+    if (k > 0 && !ll_mma_wait(a, w)) {  // the products of k - 1 have read the operands
+      cp_async_wait_group<0>();
+      return false;
+    }
+    const long long c1 = LLCLK();
+    LLPROF(3, c1 - c0);
+    {
+      tc::TileShare<THREADS> s;
+      ll_share_from_raw(st, s);
+      tc::store_share_split<THREADS>(s, 128, 0, Ahi, Alo);
+      if (two) {
+        ll_share_from_raw(st + NB * NB, s);
+        tc::store_share_split<THREADS>(s, 128, 64, Ahi, Alo);
+      }
+      ll_share_from_raw(st + 2 * NB * NB, s);
+      tc::store_share_split<THREADS>(s, 64, 0, Bhi, Blo);
+    }
+    tc::fence_proxy_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      tc::issue_product(w.tmem, tc::smem_u32(Ahi), tc::smem_u32(Alo), tc::smem_u32(Bhi), tc::smem_u32(Blo),
+                        k > 0 ? 1u : 0u);
+      tc::mma_commit(w.mbar);
+    }
+    c0 = LLCLK();
+    LLPROF(4, c0 - c1);
+    if (k + 2 < j) {
+      // every thread is past its reads of this stage (the barrier above)
+      if (!ll_wait_rows(a, a.fin, rows, 7u, k + 3, seen, s_ok)) {
+        cp_async_wait_group<0>();
+        ll_mma_wait(a, w);  // drain the products in flight before the TMEM goes
+        return false;
+      }
+      ll_fetch_step(a, i, two, j, k + 2, st);
+      LLPROF(2, LLCLK() - c0);
+    }
+  }
+  c0 = LLCLK();
+  if (!ll_mma_wait(a, w)) return false;
+  LLPROF(3, LLCLK() - c0);
+  // P from TMEM into shared memory, row m = TMEM lane
+  const int warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
+  const int m = 32 * q + lane;
+  if (two || q < 2) {  // warp-uniform
+    float v[32];
+    tc::tmem_ld32(w.tmem + ((uint32_t)(32 * q) << 16) + 32 * g, v);
+    float* dst = reinterpret_cast<float*>(w.base) + (size_t)m * LDA + 32 * g;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      *reinterpret_cast<float4*>(dst + 4 * u) = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  return true;
+}
+
+// U = A - P for rows i (and i + 1) of column j, coalesced 16-byte reads of A
+// (a row of 64 per 16 threads); into the [64][LDA] tiles U0 / U1 in shared
+// memory, or in place into A when to_global.  P is absent for j = 0.
+__device__ __forceinline__ void ll_difference(const DFArgs& a, int i, int j, bool two, const float* Ps, float* U0,
+                                              float* U1, bool to_global) {
+  for (int e = threadIdx.x; e < (two ? 128 : 64) * 16; e += THREADS) {
+    const int row = e >> 4, c4 = e & 15;
+    float4* gp = reinterpret_cast<float4*>(tile<float>(a, i + (row >> 6), j) + (size_t)(row & 63) * a.ld) + c4;
+    float4 cv = __ldcg(gp);
+    if (j > 0) {
+      const float4 pv = *reinterpret_cast<const float4*>(Ps + (size_t)row * LDA + 4 * c4);
+      cv.x -= pv.x;
+      cv.y -= pv.y;
+      cv.z -= pv.z;
+      cv.w -= pv.w;
+    }
+    if (to_global) *gp = cv;
+    else *reinterpret_cast<float4*>((row < 64 ? U0 : U1) + (row & 63) * LDA + 4 * c4) = cv;
+  }
+}
+
+// One task of the left-looking list (kinds in cholesky_replica_tasks).
+// Returns false if the run was aborted (nothing of this CTA in flight then).
+__device__ bool ll_task(const DFArgs& a, int kind, int i, int j, LLWorker& w, int* seen, int* s_ok) {
+  const int tid = threadIdx.x;
+  const bool two = i + 1 < a.nt;
+  const int rows[3] = {i, two ? i + 1 : i, j};
+  if (tid < 3) seen[tid] = 0;
+  float* Ps = reinterpret_cast<float*>(w.base);
+  float* U0 = reinterpret_cast<float*>(w.base + LL_U0);
+  float* U1 = reinterpret_cast<float*>(w.base + LL_U1);
+  long long c0 = LLCLK();
+  LLPROF(0, 1);
+  LLPROF(1, j);
+  if (kind != LL_SOLVE) {
+    if (j > 0 && !ll_products(a, i, j, w, seen, s_ok)) return false;
+    c0 = LLCLK();
+    ll_difference(a, i, j, two, Ps, U0, U1, kind == LL_UPDATE);
+    __syncthreads();
+    LLPROF(5, LLCLK() - c0);
+    c0 = LLCLK();
+  }
+  float acc[16];
+  if (kind == LL_DIAG) {
+    // F(j) over P's bytes (no longer read), then S(j + 1, j) with inv(L_jj)
+    // where factor_task_f32 left it
+    LLPROF(11, 1);
+    smem_to_acc(U0, acc);
+    factor_task_f32(a, j, acc, w.base);
+    publish(a.fin + j, j + 1);
+    if (two) {
+      solve_by_inverse(U1, reinterpret_cast<const float*>(w.base) + NB * LDA, acc);
+      store_acc(tile<float>(a, j + 1, j), a.ld, acc);
+      publish(a.fin + j + 1, j + 1);
+    }
+    LLPROF(6, LLCLK() - c0);
+  } else if (kind == LL_UPDATE) {
+    // U_ij (and U_{i+1,j}) stay in A's tiles for the solve task
+    if (tid == 0) {
+      st_release(a.upd + i, j + 1);
+      if (two) st_release(a.upd + i + 1, j + 1);
+    }
+  } else {
+    if (!ll_wait_rows(a, a.upd, rows, two ? 3u : 1u, j + 1, seen, s_ok)) return false;  // U_ij in A
+    if (!ll_wait_rows(a, a.fin, rows, 4u, j + 1, seen, s_ok)) return false;             // F(j)
+    LLPROF(7, LLCLK() - c0);
+    c0 = LLCLK();
+    float* Xs = reinterpret_cast<float*>(w.base);
+    stage_async(reinterpret_cast<const float*>(a.invdiag) + (size_t)j * NB * NB, NB, Xs, LDA);
+    stage_async(tile<float>(a, i, j), a.ld, U0, LDA);
+    if (two) stage_async(tile<float>(a, i + 1, j), a.ld, U1, LDA);
+    cp_async_wait_all();
+    __syncthreads();
+    solve_by_inverse(U0, Xs, acc);
+    store_acc(tile<float>(a, i, j), a.ld, acc);
+    if (two) {
+      solve_by_inverse(U1, Xs, acc);
+      store_acc(tile<float>(a, i + 1, j), a.ld, acc);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      st_release(a.fin + i, j + 1);
+      if (two) st_release(a.fin + i + 1, j + 1);
+    }
+    LLPROF(8, LLCLK() - c0);
+  }
+  __syncthreads();  // the next task overwrites the shared memory
+  return true;
+}
+
+// One CTA per SM (192 KB of shared memory, 64 TMEM columns), all co-resident
+// (cooperative launch).
+__global__ void __launch_bounds__(THREADS, 1) chol_batch_ll_kernel(const CholRep* __restrict__ reps,
+                                                                   const int4* __restrict__ tasks, int ntasks,
+                                                                   int* ctl) {
+  extern __shared__ __align__(1024) unsigned char ll_smem[];
+  unsigned char* smem = ll_smem;
+  if (tc::smem_u32(smem) & 1023u) {
+    // the operands need a 1024-byte aligned start: give up on the whole run,
+    // every replica reported as not factored (info -1)
+    if (threadIdx.x == 0) {
+      atomicExch(ctl + 1, 1);
+      atomicOr(reinterpret_cast<unsigned*>(ctl + 3), PBG_DEV_ERR_BARRIER);
+    }
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += gridDim.x * blockDim.x)
+      atomicCAS(reps[tasks[t].x >> 3].info, 0, -1);
+    return;
+  }
+  LLShared* sh = reinterpret_cast<LLShared*>(smem + LL_SHARED_OFFSET);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&sh->mbar, 1);
+    sh->ok = 1;
+  }
+  if (threadIdx.x < 32) tc::tmem_alloc(&sh->tmem, 64);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  LLWorker w;
+  w.mbar = &sh->mbar;
+  w.tmem = sh->tmem;
+  w.phase = 0;
+  w.base = smem;
+  const long long k0 = LLCLK();
+  while (true) {
+    const long long f0 = LLCLK();
+    if (threadIdx.x == 0) sh->task = ld_acquire(ctl + 1) ? ntasks : atomicAdd(ctl, 1);
+    __syncthreads();
+    const int t = sh->task;
+    __syncthreads();
+    LLPROF(9, LLCLK() - f0);
+    if (t >= ntasks) break;
+    const int4 tk = tasks[t];
+    const DFArgs a = batch_args(reps[tk.x >> 3], tasks, ntasks, ctl);
+    if (!ll_task(a, tk.x & 7, tk.y, tk.z, w, sh->seen, &sh->ok)) break;
+  }
+  LLPROF(10, LLCLK() - k0);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x < 32) tc::tmem_dealloc(w.tmem, 64);
+}
+
 std::mutex g_task_mu;
 std::map<int, std::pair<int4*, int>> g_task_tables;
 
@@ -2007,6 +2424,10 @@ extern "C" __attribute__((visibility("default"))) int pbg_task_trace(long long* 
   PBG_CUDA_TRY(cudaMemcpyFromSymbol(host, g_task_trace, sizeof(long long) * 4 * ntasks));
   return PBG_OK;
 }
+extern "C" __attribute__((visibility("default"))) int pbg_ll_profile(long long* host, int ctas) {
+  PBG_CUDA_TRY(cudaMemcpyFromSymbol(host, g_ll_prof, sizeof(long long) * 16 * ctas));
+  return PBG_OK;
+}
 extern "C" __attribute__((visibility("default"))) int pbg_chain_trace(long long* host, int nt) {
   PBG_CUDA_TRY(cudaMemcpyFromSymbol(host, g_chain_trace, sizeof(long long) * 8 * nt));
   return PBG_OK;
@@ -2053,10 +2474,28 @@ int launch_cholesky_df(void* A, int n, int ld, int precision, int* info, void* i
 // whole update phase to finish.  F(k+1) and U(., ., k) depend only on block
 // k-1; S(., k+1) on F(k+1) and block k-1: every task depends only on earlier
 // tasks.  The tasks carry replica tag 0; the merge writes the replica index.
-void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start) {
+//
+// The mixed-precision lists are left-looking (chol_batch_ll_kernel), two
+// segments per column j: LL_DIAG for rows (j, j + 1) and LL_UPDATE for the
+// row pairs (j + 2, j + 3), (j + 4, j + 5), ...; then LL_SOLVE for the same
+// pairs.  Merged by segment number, every replica's solves of column j come
+// after every replica's updates of column j, so F(j) has had that phase to
+// finish; column j + 1's tasks need column j's solves and come after them.
+void cholesky_replica_tasks(int nt, int precision, std::vector<int4>& tasks, std::vector<int>& seg_start) {
   tasks.clear();
   seg_start.clear();
   if (nt < 1) return;
+  if (precision != PBG_PREC_FP64) {
+    for (int j = 0; j < nt; ++j) {
+      seg_start.push_back((int)tasks.size());
+      tasks.push_back(make_int4(LL_DIAG, j, j, 0));
+      for (int i = j + 2; i < nt; i += 2) tasks.push_back(make_int4(LL_UPDATE, i, j, 0));
+      seg_start.push_back((int)tasks.size());
+      for (int i = j + 2; i < nt; i += 2) tasks.push_back(make_int4(LL_SOLVE, i, j, 0));
+    }
+    seg_start.push_back((int)tasks.size());
+    return;
+  }
   seg_start.push_back(0);
   tasks.push_back(make_int4(TASK_F, 0, 0, 0));
   for (int i = 1; i < nt; ++i) tasks.push_back(make_int4(TASK_S, i, 0, 0));
@@ -2075,11 +2514,11 @@ void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& 
   seg_start.push_back((int)tasks.size());
 }
 
-int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
-                          int ctas_per_sm, cudaStream_t st) {
-  if (ntasks <= 0) return PBG_OK;
+// Resident CTAs per SM of the batched factorisation kernel of this
+// precision (the occupancy query, once per precision) and the SM count.
+int cholesky_batch_residency(int precision, int* ctas_per_sm, int* sms) {
   const bool f64 = precision == PBG_PREC_FP64;
-  const size_t smem = f64 ? batch_smem_bytes<double>() : batch_smem_bytes<float>();
+  const size_t smem = f64 ? batch_smem_bytes<double>() : ll_smem_bytes();
   static int blocks_per_sm[2] = {-1, -1};
   static int num_sms = 0;
   int& bps = blocks_per_sm[f64 ? 0 : 1];
@@ -2087,19 +2526,33 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
     int dev;
     PBG_CUDA_TRY(cudaGetDevice(&dev));
     PBG_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+    int b = 0;
     if (f64) {
       PBG_CUDA_TRY(cudaFuncSetAttribute(chol_batch_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, chol_batch_kernel<double>, THREADS, smem));
+      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, chol_batch_kernel<double>, THREADS, smem));
     } else {
-      PBG_CUDA_TRY(cudaFuncSetAttribute(chol_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, chol_batch_kernel<float>, THREADS, smem));
+      PBG_CUDA_TRY(cudaFuncSetAttribute(chol_batch_ll_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PBG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, chol_batch_ll_kernel, THREADS, smem));
     }
-    if (bps < 1) {
+    if (b < 1) {
       pbg_set_error_message("batched cholesky kernel does not fit on an SM");
-      bps = -1;
       return PBG_ERR_CUDA;
     }
+    bps = b;
   }
+  *ctas_per_sm = bps;
+  *sms = num_sms;
+  return PBG_OK;
+}
+
+int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,
+                          int ctas_per_sm, cudaStream_t st) {
+  if (ntasks <= 0) return PBG_OK;
+  const bool f64 = precision == PBG_PREC_FP64;
+  const size_t smem = f64 ? batch_smem_bytes<double>() : ll_smem_bytes();
+  int bps = 0, num_sms = 0;
+  int rc = cholesky_batch_residency(precision, &bps, &num_sms);
+  if (rc) return rc;
   int grid = num_sms * (ctas_per_sm > 0 ? std::min(ctas_per_sm, bps) : bps);
   if (grid > ntasks) grid = ntasks;
   cudaLaunchConfig_t cfg = {};
@@ -2113,7 +2566,24 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (f64) PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<double>, reps, tasks, ntasks, ctl));
-  else PBG_CUDA_TRY(cudaLaunchKernelEx(&cfg, chol_batch_kernel<float>, reps, tasks, ntasks, ctl));
+  else {
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, chol_batch_ll_kernel, reps, tasks, ntasks, ctl);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+      // say what the asked-for residency would need
+      cudaGetLastError();
+      size_t avail = 0;
+      cudaFuncAttributes fa = {};
+      cudaOccupancyAvailableDynamicSMemPerBlock(&avail, chol_batch_ll_kernel, grid / num_sms, THREADS);
+      cudaFuncGetAttributes(&fa, chol_batch_ll_kernel);
+      cudaGetLastError();
+      pbg_set_error_message(
+          "batched factorisation: %d CTAs per SM do not fit (%zu bytes of dynamic shared memory per CTA, %zu "
+          "available at that residency; %d registers per thread, %zu bytes static shared memory)",
+          grid / num_sms, smem, avail, fa.numRegs, fa.sharedSizeBytes);
+      return PBG_ERR_CUDA;
+    }
+    PBG_CUDA_TRY(e);
+  }
   PBG_CHECK_LAUNCH();
   return PBG_OK;
 }

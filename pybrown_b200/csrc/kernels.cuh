@@ -170,7 +170,9 @@ struct CholRep {
 // One replica's task list (task.x = type, replica tag 0) cut into segments
 // that a batch interleaves with the other replicas' (see cholesky_df.cu);
 // task.x = type | replica << 3 in the merged list.
-void cholesky_replica_tasks(int nt, std::vector<int4>& tasks, std::vector<int>& seg_start);
+void cholesky_replica_tasks(int nt, int precision, std::vector<int4>& tasks, std::vector<int>& seg_start);
+// Resident CTAs per SM of the batched factorisation kernel, and the SM count.
+int cholesky_batch_residency(int precision, int* ctas_per_sm, int* sms);
 // ctl: 4 ints (next task, abort, spin failures, error bits), zero before the launch.
 // ctas_per_sm: resident CTAs per SM (0 = as many as fit).
 int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks, int ntasks, int* ctl,

@@ -141,51 +141,71 @@ struct SplitTile {
   unsigned char* lo;
 };
 
+// One thread's share of a 64 x 64 FP32 tile: PER 16-byte chunks, chunk e at
+// row (tid + e NTHREADS) / 16, columns 4 ((tid + e NTHREADS) % 16) .. +3.
+template <int NTHREADS>
+struct TileShare {
+  static constexpr int PER = TILE * 16 / NTHREADS;
+  float4 v[PER];
+};
+
+// Issues the loads of this thread's share (through L2; no wait).
+template <int NTHREADS>
+__device__ __forceinline__ void load_share(const float* src, int ld, TileShare<NTHREADS>& s) {
+#pragma unroll
+  for (int e = 0; e < TileShare<NTHREADS>::PER; ++e) {
+    const int i = threadIdx.x + e * NTHREADS, r = i >> 4, c = i & 15;
+    s.v[e] = __ldcg(reinterpret_cast<const float4*>(src + (size_t)r * ld + 4 * c));
+  }
+}
+
+// Writes the hi / lo TF32 halves of this thread's share into rows
+// row0 .. row0 + 63 of the R-row K-major operands at hi and lo.
+template <int NTHREADS>
+__device__ __forceinline__ void store_share_split(const TileShare<NTHREADS>& s, int R, int row0, unsigned char* hi,
+                                                  unsigned char* lo) {
+#pragma unroll
+  for (int e = 0; e < TileShare<NTHREADS>::PER; ++e) {
+    const int i = threadIdx.x + e * NTHREADS, r = row0 + (i >> 4), c = i & 15;
+    const uint32_t off = sw128_offset(R, r, c);
+    const float x[4] = {s.v[e].x, s.v[e].y, s.v[e].z, s.v[e].w};
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      h[u] = rna_tf32(x[u]);
+      l[u] = rna_tf32(x[u] - __uint_as_float(h[u]));
+    }
+    *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+  }
+}
+
 // Loads up to MAXT 64 x 64 FP32 tiles (row stride ld) and writes their hi /
 // lo TF32 halves into the operands: every thread issues all of its loads
 // (16 bytes each, through L2) before the first conversion, so the tiles cost
 // one memory round trip together.  All NTHREADS threads of the CTA call it.
 template <int NTHREADS, int MAXT>
 __device__ __forceinline__ void split_tiles_all(const SplitTile (&t)[MAXT], int count, int ld) {
-  constexpr int PER = TILE * 16 / NTHREADS;
-  float4 v[MAXT][PER];
+  TileShare<NTHREADS> v[MAXT];
 #pragma unroll
   for (int q = 0; q < MAXT; ++q)
-    if (q < count)
-#pragma unroll
-      for (int e = 0; e < PER; ++e) {
-        const int i = threadIdx.x + e * NTHREADS, r = i >> 4, c = i & 15;
-        v[q][e] = __ldcg(reinterpret_cast<const float4*>(t[q].src + (size_t)r * ld + 4 * c));
-      }
+    if (q < count) load_share<NTHREADS>(t[q].src, ld, v[q]);
 #pragma unroll
   for (int q = 0; q < MAXT; ++q)
-    if (q < count)
-#pragma unroll
-      for (int e = 0; e < PER; ++e) {
-        const int i = threadIdx.x + e * NTHREADS, r = t[q].row0 + (i >> 4), c = i & 15;
-        const uint32_t off = sw128_offset(t[q].R, r, c);
-        const float x[4] = {v[q][e].x, v[q][e].y, v[q][e].z, v[q][e].w};
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          h[u] = rna_tf32(x[u]);
-          l[u] = rna_tf32(x[u] - __uint_as_float(h[u]));
-        }
-        *reinterpret_cast<uint4*>(t[q].hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(t[q].lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-      }
+    if (q < count) store_share_split<NTHREADS>(v[q], t[q].R, t[q].row0, t[q].hi, t[q].lo);
 }
 
 // Issues P = A_hi B_hi + A_hi B_lo + A_lo B_hi (M = 128, N = 64, K = 64) into
-// the TMEM accumulator d_tmem, from zero.  One thread.
+// the TMEM accumulator d_tmem: from zero, or added to it with accumulate = 1.
+// One thread.
 __device__ __forceinline__ void issue_product(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
-                                              uint32_t b_lo) {
+                                              uint32_t b_lo, uint32_t accumulate = 0) {
   constexpr uint32_t idesc = idesc_tf32(128, 64);
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     const uint32_t ka = (uint32_t)((s >> 2) * 128 * 128 + (s & 3) * 32);  // A: 128 rows per K block
     const uint32_t kb = (uint32_t)((s >> 2) * 64 * 128 + (s & 3) * 32);   // B: 64 rows per K block
-    mma_tf32(d_tmem, sw128_desc(a_hi + ka), sw128_desc(b_hi + kb), idesc, s > 0 ? 1u : 0u);
+    mma_tf32(d_tmem, sw128_desc(a_hi + ka), sw128_desc(b_hi + kb), idesc, s > 0 ? 1u : accumulate);
     mma_tf32(d_tmem, sw128_desc(a_hi + ka), sw128_desc(b_lo + kb), idesc, 1u);
     mma_tf32(d_tmem, sw128_desc(a_lo + ka), sw128_desc(b_hi + kb), idesc, 1u);
   }

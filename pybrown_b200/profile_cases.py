@@ -76,6 +76,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("fp64", "mixed", "mixed_fp64_diag"), default="mixed",
                     help="mixed_fp64_diag: cholesky only, the FP32 factorisation with FP64 diagonal tiles")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--merge-order", default="larger_first", help="batch: task merge order")
+    ap.add_argument("--ctas", type=int, default=0, help="batch: factorisation CTAs per SM (0 = as many as fit)")
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return _batch(a, torch)
@@ -124,8 +126,10 @@ def _batch(a, torch):
         radii = rng.uniform(10.0, 30.0, size=int(N))
         L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
         batch.add(place_beads(rng, radii, L), radii, L, seed=k, noise="device")
+    batch.set_schedule(a.merge_order, a.ctas)
     t = _time(torch, lambda: batch.propagate(0.5), a.reps)
-    print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}): {_ms(t)} per step")
+    print(f"batch {a.replicas} replicas ({int(Ns.sum())} beads, {a.precision}, {a.merge_order}, "
+          f"{a.ctas or 'max'} CTAs/SM): {_ms(t)} per step")
     batch.close()
 
 
