@@ -1673,26 +1673,18 @@ __global__ void __launch_bounds__(THREADS, 1) chol_df_kernel(DFArgs a) {
   }
 }
 
-// Batched factorisation: every task comes from the shared list (there is no
-// chain CTA); F(k) applies its last update itself.  Shared memory: two T
-// tiles (sA, sB) for the updates and solves; F uses two FP64 tiles (L_kk,
-// inverse) over the same bytes and the FP64 factor scratch after them.
-template <typename T>
+// Batched FP64 factorisation (right-looking; the mixed batch runs the
+// left-looking chol_batch_ll_kernel below): every task comes from the shared
+// list (there is no chain CTA); F(k) applies its last update itself.  Shared
+// memory: two tiles (sA, sB) for the updates and solves; F uses two tiles
+// (L_kk, inverse) over the same bytes and the factor scratch after them.
 constexpr size_t batch_smem_bytes() {
   // an F task's factor scratch, or a paired update's five tiles
-  if constexpr (sizeof(T) == 8) return std::max(sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>()),
-                                                5 * NB * LDA * sizeof(T));
-  else return std::max(factor_task_f32_smem_bytes(), 5 * NB * LDA * sizeof(T));
+  return std::max(sizeof(double) * (2 * NB * LDA + factor_smem_elems<double>()), 5 * NB * LDA * sizeof(double));
 }
 
-// The batched kernel's task loop.  The mixed path's F tasks factor and invert
-// in FP32 like the single-matrix FP32 chain.  Its updates stay 3xTF32
-// `mma.sync` products in pairs: with tcgen05 tasks (update_rows_tc, one row
-// pair per task) the 256-replica factorisation took 7.8 ms against 4.7 ms --
-// each task waits for its own MMAs and pays two memory round trips (operands,
-// then C), where the mma.sync task stages all five tiles in one round and
-// overlaps its loads with the math inside the CTA, and the batch runs two
-// CTAs per SM to hide what is left.
+// The FP64 batched kernel's task loop: DMMA updates in pairs (five tiles
+// staged in one round, the loads overlapped with the math inside the CTA).
 template <typename T>
 __device__ void batch_worker_loop(const CholRep* __restrict__ reps, const int4* __restrict__ tasks, int ntasks,
                                   int* ctl, unsigned char* smem) {
@@ -1731,12 +1723,8 @@ __device__ void batch_worker_loop(const CholRep* __restrict__ reps, const int4* 
       const int* fl[3] = {a.fin + i * nt + k, a.fin + j * nt + k, a.upd + i * nt + j};
       const int tg[3] = {1, 1, k};
       if (!wait_all(a, fl, tg, 3, &s_ok)) return;
-      if constexpr (sizeof(T) == 4) {
-        update_tile(a, i, j, k, acc, sA, sB, sB + NB * LDA);  // three FP32 tiles fit the FP64 layout
-      } else {
-        load_and_update(a, i, j, k, acc, sA, sB);
-        store_acc(tile<T>(a, i, j), a.ld, acc);
-      }
+      load_and_update(a, i, j, k, acc, sA, sB);
+      store_acc(tile<T>(a, i, j), a.ld, acc);
       publish(a.upd + i * nt + j, k + 1);
     } else if (type == TASK_U2) {
       const int* fl[5] = {a.fin + i * nt + k, a.fin + (i + 1) * nt + k, a.fin + j * nt + k, a.upd + i * nt + j,
@@ -1760,8 +1748,7 @@ __device__ void batch_worker_loop(const CholRep* __restrict__ reps, const int4* 
         load_acc(tile<T>(a, i, col), a.ld, acc);
       }
       if (type == TASK_F) {
-        if constexpr (sizeof(T) == 8) factor_tile<double>(a, col, acc, fs64, Lk64, X64);
-        else factor_task_f32(a, col, acc, smem);
+        factor_tile<double>(a, col, acc, fs64, Lk64, X64);
       } else {
         if (!wait_geq(a, a.fin + col * nt + col, 1, &s_ok)) return;
         stage_async(reinterpret_cast<const T*>(a.invdiag) + (size_t)col * NB * NB, NB, sB, LDA);
@@ -1777,13 +1764,11 @@ __device__ void batch_worker_loop(const CholRep* __restrict__ reps, const int4* 
   }
 }
 
-// Two CTAs per SM in the mixed path: a second task in flight per SM hides
-// L2 latency (measured 9.8 ms against 12.4 ms for a 256-replica step at one
-// CTA per SM).  One CTA per SM in the FP64 path.
 template <typename T>
-__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 2 : 1) chol_batch_kernel(const CholRep* __restrict__ reps,
+__global__ void __launch_bounds__(THREADS, 1) chol_batch_kernel(const CholRep* __restrict__ reps,
                                                                  const int4* __restrict__ tasks, int ntasks,
                                                                  int* ctl) {
+  static_assert(sizeof(T) == 8, "the mixed batch runs chol_batch_ll_kernel");
   extern __shared__ __align__(16) unsigned char smem[];
   batch_worker_loop<T>(reps, tasks, ntasks, ctl, smem);
 }
@@ -2518,7 +2503,7 @@ void cholesky_replica_tasks(int nt, int precision, std::vector<int4>& tasks, std
 // precision (the occupancy query, once per precision) and the SM count.
 int cholesky_batch_residency(int precision, int* ctas_per_sm, int* sms) {
   const bool f64 = precision == PBG_PREC_FP64;
-  const size_t smem = f64 ? batch_smem_bytes<double>() : ll_smem_bytes();
+  const size_t smem = f64 ? batch_smem_bytes() : ll_smem_bytes();
   static int blocks_per_sm[2] = {-1, -1};
   static int num_sms = 0;
   int& bps = blocks_per_sm[f64 ? 0 : 1];
@@ -2549,7 +2534,7 @@ int launch_cholesky_batch(int precision, const CholRep* reps, const int4* tasks,
                           int ctas_per_sm, cudaStream_t st) {
   if (ntasks <= 0) return PBG_OK;
   const bool f64 = precision == PBG_PREC_FP64;
-  const size_t smem = f64 ? batch_smem_bytes<double>() : ll_smem_bytes();
+  const size_t smem = f64 ? batch_smem_bytes() : ll_smem_bytes();
   int bps = 0, num_sms = 0;
   int rc = cholesky_batch_residency(precision, &bps, &num_sms);
   if (rc) return rc;
