@@ -393,7 +393,11 @@ PBG_API int pbg_batch_check_factor(pbg_batch *b, int slot, int *info, void *stre
 /* Schedule of the batched factorisation (no counterpart in the reference).
  * merge_order: how the replicas' task segments are interleaved in the one
  * task list; ctas_per_sm: resident CTAs per SM of the persistent kernel
- * (0 = as many as fit).  No choice changes any result bit. */
+ * (0 = as many as fit; a larger count is cut to what fits).  No choice
+ * changes any result bit.  The mixed batch factors left-looking (tasks per
+ * column: the diagonal pair and the updates, then the solves), the FP64 batch
+ * right-looking (tasks per panel: F, updates, solves); the segments merged are
+ * those. */
 enum {
   PBG_MERGE_LARGER_FIRST = 0,
   PBG_MERGE_ADDED = 1,
@@ -410,7 +414,8 @@ enum {
 PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_sm);
 /* Autotuner: after a step has built D (not inside a step), times `reps`
  * factorisations of the current matrices under every schedule (the
- * PBG_MERGE_ORDERS merge orders x 1 or 2 CTAs per SM in FP32, 1 in FP64),
+ * PBG_MERGE_ORDERS merge orders x 1 .. min(2, the kernel's residency) CTAs
+ * per SM),
  * keeps the fastest and leaves B as the factor of the current D (the value a
  * step would give).  best[2] = {merge_order, ctas_per_sm}; ms (may be NULL)
  * receives the mean time of each candidate, merge order major
