@@ -1804,7 +1804,7 @@ constexpr uint32_t LL_OPERAND_BYTES = 2 * LL_A_BYTES + 2 * LL_B_BYTES;
 // floats from 0), the U tiles ([64][LDA] at LL_U0 and LL_U1) and the factor
 // scratch (from 0).
 struct LLShared {
-  uint64_t mbar;
+  uint64_t mbar, conv;
   uint32_t tmem;
   int task, ok, seen[3];
 };
@@ -1821,8 +1821,10 @@ static_assert(LL_U1 + sizeof(float) * NB * LDA <= LL_OPERAND_BYTES, "U1 lies out
 
 struct LLWorker {
   uint64_t* mbar;       // completion of the products of one K-step
+  uint64_t* conv;       // every thread's operands of a K-step written (THREADS arrivals)
   uint32_t tmem;        // TMEM base: the 128 x 64 FP32 accumulator
   uint32_t phase;
+  uint32_t conv_phase;  // thread 0's
   unsigned char* base;  // 1024-byte aligned operand area
 };
 
@@ -1894,21 +1896,6 @@ __device__ bool ll_wait_rows(const DFArgs& a, const int* base, const int (&rows)
   return *s_ok != 0;
 }
 
-// Waits (bounded) for the products of the last commit; one verdict for the
-// CTA.  A failure aborts the run like an expired flag wait.
-__device__ bool ll_mma_wait(const DFArgs& a, LLWorker& w) {
-  bool ok = tc::mbar_wait(w.mbar, w.phase, a.spin_limit);
-  if (!ok) ok = tc::mbar_wait(w.mbar, w.phase, a.spin_limit);  // the MMAs must not outlive the TMEM
-  ok = __syncthreads_and(ok) != 0;
-  w.phase ^= 1;
-  if (!ok && threadIdx.x == 0) {
-    atomicExch(a.ctl + 1, 1);
-    atomicOr(a.err, PBG_DEV_ERR_BARRIER);
-    atomicCAS(a.info, 0, -1);
-  }
-  tc::fence_after_sync();
-  return ok;
-}
 
 // cp.async (16 bytes, through L2) of this thread's share of a 64 x 64 FP32
 // tile into a row-major [64][64] stage; the same thread converts the same
@@ -1943,13 +1930,51 @@ __device__ __forceinline__ void ll_share_from_raw(const float* raw, tc::TileShar
   }
 }
 
+// Per-thread bounded wait until base[rows[q]] >= target for q = 0, 1, 2,
+// with the counts observed so far kept in the thread's registers (seen): a
+// wait that an earlier observation satisfies costs nothing, and the thread's
+// own acquire orders its later reads (no barrier).  false: the wait gave up
+// (recorded like an expired wait_all) or the run was aborted.
+__device__ bool ll_thread_wait_rows(const DFArgs& a, const int* base, const int (&rows)[3], int target,
+                                    int (&seen)[3]) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    for (long long it = 0; seen[q] < target; ++it) {
+      const int v = ld_acquire(base + rows[q]);
+      if (v >= target) {
+        seen[q] = v;
+        break;
+      }
+      if ((it & 63) == 63) {
+        if (ld_acquire(a.ctl + 1)) return false;
+        if (it > a.spin_limit) {
+          atomicExch(a.ctl + 1, 1);
+          atomicAdd(a.ctl + 2, 1);
+          atomicOr(a.err, PBG_DEV_ERR_BARRIER);
+          atomicCAS(a.info, 0, -1);
+          return false;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void ll_arrive(uint64_t* m) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(m)) : "memory");
+}
+
 // P = sum_{k < j} [L_ik; L_{i+1,k}] L_jk^T into shared memory ([128][LDA]
 // floats at the operand area's start), for j > 0.  The tiles of K-step k + 2
-// are fetched (cp.async, two raw stages) while the products of k run and
-// the tiles of k + 1 wait converted-to-be; the rows' counters are waited for
-// before each fetch.  Returns false if the run was aborted (nothing of this
-// CTA in flight then).
-__device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* seen, int* s_ok) {
+// are fetched (cp.async, two raw stages) while the products of k run.  No
+// CTA barrier inside the K loop: every thread fetches and converts only its
+// own chunks (so the raw stages need no hand-over), waits for the previous
+// products on their mbarrier before overwriting the operands, and arrives on
+// the conversion mbarrier; thread 0 waits for all arrivals and issues the
+// MMAs.  Returns false (after a CTA barrier) if the run was aborted, with no
+// products of this CTA left in flight.
+__device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
   const int tid = threadIdx.x;
   const bool two = i + 1 < a.nt;
   unsigned char* Ahi = w.base;
@@ -1959,6 +1984,7 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* see
   float* raw[2] = {reinterpret_cast<float*>(w.base + LL_OPERAND_BYTES),
                    reinterpret_cast<float*>(w.base + LL_OPERAND_BYTES + LL_RAW_BYTES)};
   const int rows[3] = {i, two ? i + 1 : i, j};
+  int seen[3] = {0, 0, 0};
   if (!two) {
     // rows 64 .. 127 of both A halves stay zero for the whole task: bytes
     // 8192 .. 16383 of each of the two K blocks (16384 bytes each)
@@ -1969,14 +1995,13 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* see
     }
   }
   long long c0 = LLCLK();
-  if (!ll_wait_rows(a, a.fin, rows, 7u, 1, seen, s_ok)) return false;
-  ll_fetch_step(a, i, two, j, 0, raw[0]);
+  bool ok = ll_thread_wait_rows(a, a.fin, rows, 1, seen);
+  if (ok) ll_fetch_step(a, i, two, j, 0, raw[0]);
+  else cp_async_commit();
   if (j > 1) {
-    if (!ll_wait_rows(a, a.fin, rows, 7u, 2, seen, s_ok)) {
-      cp_async_wait_group<0>();
-      return false;
-    }
-    ll_fetch_step(a, i, two, j, 1, raw[1]);
+    ok = ok && ll_thread_wait_rows(a, a.fin, rows, 2, seen);
+    if (ok) ll_fetch_step(a, i, two, j, 1, raw[1]);
+    else cp_async_commit();
   }
   LLPROF(2, LLCLK() - c0);
   for (int k = 0; k < j; ++k) {
@@ -1984,9 +2009,10 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* see
     c0 = LLCLK();
     if (k + 1 < j) cp_async_wait_group<1>();
     else cp_async_wait_group<0>();
-    if (k > 0 && !ll_mma_wait(a, w)) {  // the products of k - 1 have read the operands
-      cp_async_wait_group<0>();
-      return false;
+    if (k > 0) {  // the products of k - 1 have read the operands
+      if (!tc::mbar_wait(w.mbar, w.phase, a.spin_limit)) ok = false;
+      w.phase ^= 1;
+      tc::fence_after_sync();
     }
     const long long c1 = LLCLK();
     LLPROF(3, c1 - c0);
@@ -2002,8 +2028,10 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* see
       tc::store_share_split<THREADS>(s, 64, 0, Bhi, Blo);
     }
     tc::fence_proxy_smem();
-    __syncthreads();
+    ll_arrive(w.conv);
     if (tid == 0) {
+      if (!tc::mbar_wait(w.conv, w.conv_phase, a.spin_limit)) ok = false;  // every thread's operands written
+      w.conv_phase ^= 1;
       tc::fence_after_sync();
       tc::issue_product(w.tmem, tc::smem_u32(Ahi), tc::smem_u32(Alo), tc::smem_u32(Bhi), tc::smem_u32(Blo),
                         k > 0 ? 1u : 0u);
@@ -2012,19 +2040,26 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w, int* see
     c0 = LLCLK();
     LLPROF(4, c0 - c1);
     if (k + 2 < j) {
-      // every thread is past its reads of this stage (the barrier above)
-      if (!ll_wait_rows(a, a.fin, rows, 7u, k + 3, seen, s_ok)) {
-        cp_async_wait_group<0>();
-        ll_mma_wait(a, w);  // drain the products in flight before the TMEM goes
-        return false;
-      }
-      ll_fetch_step(a, i, two, j, k + 2, st);
+      ok = ok && ll_thread_wait_rows(a, a.fin, rows, k + 3, seen);
+      if (ok) ll_fetch_step(a, i, two, j, k + 2, st);
+      else cp_async_commit();
       LLPROF(2, LLCLK() - c0);
     }
   }
   c0 = LLCLK();
-  if (!ll_mma_wait(a, w)) return false;
+  if (!tc::mbar_wait(w.mbar, w.phase, a.spin_limit)) ok = false;
+  w.phase ^= 1;
+  ok = __syncthreads_and(ok) != 0;
   LLPROF(3, LLCLK() - c0);
+  if (!ok) {
+    if (tid == 0) {
+      atomicExch(a.ctl + 1, 1);
+      atomicOr(a.err, PBG_DEV_ERR_BARRIER);
+      atomicCAS(a.info, 0, -1);
+    }
+    return false;
+  }
+  tc::fence_after_sync();
   // P from TMEM into shared memory, row m = TMEM lane
   const int warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
   const int m = 32 * q + lane;
@@ -2076,7 +2111,7 @@ __device__ bool ll_task(const DFArgs& a, int kind, int i, int j, LLWorker& w, in
   LLPROF(0, 1);
   LLPROF(1, j);
   if (kind != LL_SOLVE) {
-    if (j > 0 && !ll_products(a, i, j, w, seen, s_ok)) return false;
+    if (j > 0 && !ll_products(a, i, j, w)) return false;
     c0 = LLCLK();
     ll_difference(a, i, j, two, Ps, U0, U1, kind == LL_UPDATE);
     __syncthreads();
@@ -2152,6 +2187,7 @@ __global__ void __launch_bounds__(THREADS, 1) chol_batch_ll_kernel(const CholRep
   LLShared* sh = reinterpret_cast<LLShared*>(smem + LL_SHARED_OFFSET);
   if (threadIdx.x == 0) {
     tc::mbar_init(&sh->mbar, 1);
+    tc::mbar_init(&sh->conv, THREADS);
     sh->ok = 1;
   }
   if (threadIdx.x < 32) tc::tmem_alloc(&sh->tmem, 64);
@@ -2160,8 +2196,10 @@ __global__ void __launch_bounds__(THREADS, 1) chol_batch_ll_kernel(const CholRep
   tc::fence_after_sync();
   LLWorker w;
   w.mbar = &sh->mbar;
+  w.conv = &sh->conv;
   w.tmem = sh->tmem;
   w.phase = 0;
+  w.conv_phase = 0;
   w.base = smem;
   const long long k0 = LLCLK();
   while (true) {

@@ -167,3 +167,32 @@ def test_batch_replica_n512_vs_oracle(oracle_omp_lib, precision, tol):
     for s, box, init, L in reps[1:]:
         assert _disp_err(batch.positions(s), box.pos, init, L) <= tol, s
     batch.close()
+
+
+def test_batch_replica_n2048_mixed_vs_oracle(oracle_omp_lib):
+    """The largest request of the serving stream (2048 beads, radii
+    U[10, 40], volume fraction 0.05: 96 tile columns for the left-looking
+    batched factorisation) in a batch with a small replica, one step against
+    the oracle run alone."""
+    from oracle.oracle import OracleBox
+    from pybrown_b200.batch import ReplicaBatch
+    batch = ReplicaBatch(precision="mixed")
+    reps = []
+    for k, N in enumerate((2048, 64)):
+        rng = np.random.default_rng(950 + k)
+        radii = rng.uniform(10.0, 40.0, size=N)
+        L = float((np.sum(4.0 / 3.0 * np.pi * radii ** 3) / 0.05) ** (1.0 / 3.0))
+        pos, radii = _config(950 + k, N, L, 10.0, 40.0)
+        inp = _inp(box_length=L, seed=70 + k)
+        slot = batch.add(pos, radii, L, T=inp["T"], viscosity=inp["viscosity"], seed=inp["seed"], noise="numpy")
+        reps.append((slot, OracleBox(pos, radii, inp, clib=oracle_omp_lib), pos, L))
+    batch.propagate(1.0)
+    for s, box, init, L in reps:
+        box.propagate(1.0)
+        assert 3 * len(init) * batch.last_move_attempts(s) == box.draw_count, s
+    s, box, init, L = reps[0]
+    assert rel_err(batch.matrix(s, "D"), box.D) <= 1e-5
+    assert rel_err(np.tril(batch.matrix(s, "B")), box.B) <= 1e-5
+    for s, box, init, L in reps:
+        assert _disp_err(batch.positions(s), box.pos, init, L) <= 1e-5, s
+    batch.close()
