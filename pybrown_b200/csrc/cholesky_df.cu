@@ -2039,6 +2039,17 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
     }
     c0 = LLCLK();
     LLPROF(4, c0 - c1);
+    if (k + 1 == j) {
+      // both raw stages are consumed: A's tiles (i, j), (i + 1, j) for the
+      // difference U = A - P come in while the last products run, each
+      // thread's chunks where ll_difference reads them
+      float* As = raw[0];
+      for (int e = tid; e < (two ? 128 : 64) * 16; e += THREADS) {
+        const int row = e >> 4, c4 = e & 15;
+        cp_async16(As + row * NB + 4 * c4, tile<float>(a, i + (row >> 6), j) + (size_t)(row & 63) * a.ld + 4 * c4);
+      }
+      cp_async_commit();
+    }
     if (k + 2 < j) {
       ok = ok && ll_thread_wait_rows(a, a.fin, rows, k + 3, seen);
       if (ok) ll_fetch_step(a, i, two, j, k + 2, st);
@@ -2076,15 +2087,17 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
   return true;
 }
 
-// U = A - P for rows i (and i + 1) of column j, coalesced 16-byte reads of A
-// (a row of 64 per 16 threads); into the [64][LDA] tiles U0 / U1 in shared
-// memory, or in place into A when to_global.  P is absent for j = 0.
-__device__ __forceinline__ void ll_difference(const DFArgs& a, int i, int j, bool two, const float* Ps, float* U0,
-                                              float* U1, bool to_global) {
+// U = A - P for rows i (and i + 1) of column j, a row of 64 per 16 threads;
+// A from its prefetched copy As (row-major [128][64], j > 0) or from global
+// memory (j = 0, no P); into the [64][LDA] tiles U0 / U1 in shared memory,
+// or in place into A when to_global.
+__device__ __forceinline__ void ll_difference(const DFArgs& a, int i, int j, bool two, const float* Ps,
+                                              const float* As, float* U0, float* U1, bool to_global) {
+  if (j > 0) cp_async_wait_group<0>();  // this thread's chunks of A, fetched during the last products
   for (int e = threadIdx.x; e < (two ? 128 : 64) * 16; e += THREADS) {
     const int row = e >> 4, c4 = e & 15;
     float4* gp = reinterpret_cast<float4*>(tile<float>(a, i + (row >> 6), j) + (size_t)(row & 63) * a.ld) + c4;
-    float4 cv = __ldcg(gp);
+    float4 cv = j > 0 ? *reinterpret_cast<const float4*>(As + row * NB + 4 * c4) : __ldcg(gp);
     if (j > 0) {
       const float4 pv = *reinterpret_cast<const float4*>(Ps + (size_t)row * LDA + 4 * c4);
       cv.x -= pv.x;
@@ -2113,7 +2126,8 @@ __device__ bool ll_task(const DFArgs& a, int kind, int i, int j, LLWorker& w, in
   if (kind != LL_SOLVE) {
     if (j > 0 && !ll_products(a, i, j, w)) return false;
     c0 = LLCLK();
-    ll_difference(a, i, j, two, Ps, U0, U1, kind == LL_UPDATE);
+    ll_difference(a, i, j, two, Ps, reinterpret_cast<const float*>(w.base + LL_OPERAND_BYTES), U0, U1,
+                  kind == LL_UPDATE);
     __syncthreads();
     LLPROF(5, LLCLK() - c0);
     c0 = LLCLK();
