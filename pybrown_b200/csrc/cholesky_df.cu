@@ -1814,6 +1814,8 @@ constexpr size_t ll_smem_bytes() { return LL_SHARED_OFFSET + sizeof(LLShared); }
 static_assert(ll_smem_bytes() <= 227 * 1024, "the worker does not fit an SM");
 // task kinds of the left-looking list
 enum : int { LL_DIAG = 0, LL_UPDATE = 1, LL_SOLVE = 2 };
+// K-steps (of 64) accumulated in TMEM before the sum is added in FP32
+constexpr int LL_CHUNK = 4;
 constexpr uint32_t LL_U0 = 40960, LL_U1 = 61440;
 static_assert(factor_task_f32_smem_bytes() <= LL_U0, "the factor scratch overlaps U0");
 static_assert(sizeof(float) * 128 * LDA <= LL_U0, "P overlaps U0");
@@ -2004,6 +2006,16 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
     else cp_async_commit();
   }
   LLPROF(2, LLCLK() - c0);
+  // the products accumulate in TMEM for LL_CHUNK K-steps at a time; each
+  // chunk's sum is then added in FP32 to racc (this thread's row m, columns
+  // 32 g .. 32 g + 31), so no accumulation runs longer than K = 64 LL_CHUNK
+  // in the tensor cores
+  const int warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
+  const int m = 32 * q + lane;
+  const uint32_t tacc = w.tmem + ((uint32_t)(32 * q) << 16) + 32 * g;
+  float racc[32];
+#pragma unroll
+  for (int u = 0; u < 32; ++u) racc[u] = 0.0f;
   for (int k = 0; k < j; ++k) {
     float* st = raw[k & 1];
     c0 = LLCLK();
@@ -2013,6 +2025,15 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
       if (!tc::mbar_wait(w.mbar, w.phase, a.spin_limit)) ok = false;
       w.phase ^= 1;
       tc::fence_after_sync();
+      if (k % LL_CHUNK == 0) {
+        // a chunk is complete: fold it into racc before the next product
+        // starts the accumulator from zero (ordered by the conversion mbarrier)
+        float v[32];
+        tc::tmem_ld32(tacc, v);
+#pragma unroll
+        for (int u = 0; u < 32; ++u) racc[u] += v[u];
+        tc::fence_before_sync();
+      }
     }
     const long long c1 = LLCLK();
     LLPROF(3, c1 - c0);
@@ -2034,7 +2055,7 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
       w.conv_phase ^= 1;
       tc::fence_after_sync();
       tc::issue_product(w.tmem, tc::smem_u32(Ahi), tc::smem_u32(Alo), tc::smem_u32(Bhi), tc::smem_u32(Blo),
-                        k > 0 ? 1u : 0u);
+                        k % LL_CHUNK != 0 ? 1u : 0u);
       tc::mma_commit(w.mbar);
     }
     c0 = LLCLK();
@@ -2071,16 +2092,19 @@ __device__ bool ll_products(const DFArgs& a, int i, int j, LLWorker& w) {
     return false;
   }
   tc::fence_after_sync();
-  // P from TMEM into shared memory, row m = TMEM lane
-  const int warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
-  const int m = 32 * q + lane;
-  if (two || q < 2) {  // warp-uniform
+  // P = racc + the last chunk from TMEM, into shared memory, row m = TMEM lane
+  {
     float v[32];
-    tc::tmem_ld32(w.tmem + ((uint32_t)(32 * q) << 16) + 32 * g, v);
+    tc::tmem_ld32(tacc, v);
+#pragma unroll
+    for (int u = 0; u < 32; ++u) racc[u] += v[u];
+  }
+  if (two || q < 2) {  // warp-uniform
     float* dst = reinterpret_cast<float*>(w.base) + (size_t)m * LDA + 32 * g;
 #pragma unroll
     for (int u = 0; u < 8; ++u)
-      *reinterpret_cast<float4*>(dst + 4 * u) = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+      *reinterpret_cast<float4*>(dst + 4 * u) =
+          make_float4(racc[4 * u], racc[4 * u + 1], racc[4 * u + 2], racc[4 * u + 3]);
   }
   tc::fence_before_sync();
   __syncthreads();
