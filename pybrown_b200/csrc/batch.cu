@@ -13,8 +13,9 @@
 // steps while the others keep their state on the device.  One step is a
 // fixed sequence of launches over all replicas: phase tables and Ewald tiles
 // (one work list), the padded copy into B, one cooperative data-flow Cholesky
-// over every replica's tiles, then the per-replica vector kernels (replica =
-// blockIdx.y).  Replicas never interact, and each one's arithmetic does not
+// over every replica's tiles (left-looking on the tcgen05 tensor cores in the
+// mixed precision, right-looking DMMA tile tasks in FP64), then the
+// per-replica vector kernels (replica = blockIdx.y).  Replicas never interact, and each one's arithmetic does not
 // depend on which other replicas share the batch.
 #include <algorithm>
 #include <cmath>

@@ -1,38 +1,46 @@
 // Data-flow tiled Cholesky factorisation on sm_100a (the factor of
 // numpy.linalg.cholesky at src/bdsim/pyBrown/box.py:554).
 //
-// One persistent kernel, all CTAs co-resident (cooperative launch), one CTA
-// per SM.  The 64 x 64 tiles of the lower triangle are processed as tasks:
+// Single matrix: one persistent kernel, all CTAs co-resident (cooperative
+// launch), one CTA per SM.  The 64 x 64 tiles of the lower triangle are
+// processed as tasks:
 //   F(k)     diagonal tile k: its last update (column k-1), then the
-//            factorisation by 8-column panels (each 8 x 8 pivot block factored
-//            in registers with rsqrt pivots, rank-8 trailing updates on the
-//            tensor cores) and the explicit inverse inv(L_kk);
+//            factorisation by 8-column panels (each 8 x 8 pivot block
+//            factored in registers, rank-8 trailing updates by the other
+//            warps) and the explicit inverse inv(L_kk);
 //   S(i, k)  tile (i, k) below the diagonal: its last update, then
-//            L_ik = A_ik inv(L_kk)^T as one tensor-core tile product;
-//   U(i,j,k) trailing update A_ij -= L_ik L_jk^T (j >= k+2) on the tensor
-//            cores: FP64 DMMA (mma.sync m8n8k4 f64) in the FP64 path,
-//            3xTF32 split products (mma.sync m16n8k8 tf32, hi*hi + hi*lo +
-//            lo*hi, FP32 accumulation) in the mixed path.
-// The diagonal tiles are always factored and inverted in FP64; the mixed
-// path (FP32 matrix, 3xTF32 updates) rounds L_kk and inv(L_kk) to FP32 on store.
+//            L_ik = A_ik inv(L_kk)^T as one tile product;
+//   U(i,j,k) trailing update A_ij -= L_ik L_jk^T (j >= k+2): FP64 DMMA
+//            (mma.sync m8n8k4 f64) in the FP64 path; in the mixed path
+//            3xTF32 split products (hi*hi + hi*lo + lo*hi) on the tcgen05
+//            tensor cores, up to four rows per task, accumulated in TMEM
+//            (tc_tile.cuh).
+// The FP64 path factors and inverts the diagonal tiles in FP64; the mixed
+// path (FP32 matrix) does both in FP32 on the chain CTA (run_chain_f32), or
+// in FP64 rounded to FP32 on store (PBG_PREC_MIXED_FP64_DIAG).
 //
 // The critical path of the factorisation is F(0), S(1,0), F(1), S(2,1), ...:
 // block 0 (the chain CTA) runs exactly that sequence and keeps what one step
 // hands to the next in shared memory (L(k, k-1) for the update of F(k) and
 // S(k+1, k); inv(L_kk) for S(k+1, k)), so the chain never waits on a round
-// trip through L2.  The other CTAs take the remaining tasks
-// in a fixed order from an atomic counter: S(., 0), then for each k the
-// solves S(i, k+1) (i >= k+3) and the updates U(., ., k), the update that
-// gates the next panel first; the last update of the chain's next solve
-// S(k+2, k+1) leads the list for panel k.  Every task depends only on chain tasks and on
+// trip through L2.  The other CTAs take the remaining tasks in a fixed order
+// from an atomic counter: S(., 0), then for each k the solves S(i, k+1)
+// (i >= k+3) and the updates U(., ., k), the update that gates the next panel
+// first; the last update of the chain's next solve S(k+2, k+1) leads the list
+// for panel k.  With an output X (the SPD inverse) the same list also forms
+// X = inv(L) (XG / XZ tasks).  Every task depends only on chain tasks and on
 // tasks earlier in the list, so with all CTAs resident the lowest unfinished
 // task can always run.
 //
-// Dependencies are tracked per tile: upd[i][j] counts applied updates,
-// fin[i][j] marks a final L tile.  Waits spin on these flags with a bounded
-// iteration count; on expiry the kernel raises an abort flag, marks info = -1
-// and every CTA returns.  Tile data written by other CTAs is read with
-// L2-coherent loads (ld.global.cg, cp.async.cg).
+// Batches of independent matrices: FP64 right-looking tile tasks
+// (chol_batch_kernel<double>); mixed left-looking tasks that accumulate a
+// whole K range on the tcgen05 tensor cores (chol_batch_ll_kernel).
+//
+// Dependencies are tracked per tile (per row in the left-looking batch):
+// upd counts applied updates, fin marks final L tiles.  Waits spin on these
+// flags with a bounded iteration count; on expiry the kernel raises an abort
+// flag, marks info = -1 and every CTA returns.  Tile data written by other
+// CTAs is read with L2-coherent loads (ld.global.cg, cp.async.cg).
 #include <algorithm>
 #include <map>
 #include <mutex>
