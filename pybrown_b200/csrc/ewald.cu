@@ -50,11 +50,23 @@ template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
 __device__ __forceinline__ double d_erfc(double x) { return erfc(x); }
-__device__ __forceinline__ float d_erfc(float x) { return erfcf(x); }
 __device__ __forceinline__ double d_exp(double x) { return exp(x); }
-__device__ __forceinline__ float d_exp(float x) { return expf(x); }
 __device__ __forceinline__ double d_sqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }
+
+// erfc(x) for x >= 0 in FP32 from e = exp(-x^2), by Abramowitz & Stegun,
+// Handbook of Mathematical Functions, 7.1.26 (Hastings' rational
+// approximation): erfc(x) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-x^2}
+// with t = 1 / (1 + p x), absolute error below 1.5e-7 (a few FP32 ulps of
+// erfc's values near 1).  The real-space Ewald sum needs exp(-x^2) anyway.
+__device__ __forceinline__ float erfc_as(float x, float e) {
+  const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
+  float p = 1.061405429f;
+  p = fmaf(p, t, -1.453152027f);
+  p = fmaf(p, t, 1.421413741f);
+  p = fmaf(p, t, -0.284496736f);
+  p = fmaf(p, t, 0.254829592f);
+  return p * t * e;
+}
 
 // Free-space RPY pair block in FP64 (diff_tensor.c:490-549), three regimes.
 __device__ void rpy_pair_fp64(double ai, double aj, double rx, double ry, double rz, double out[6]) {
@@ -123,14 +135,28 @@ __device__ __forceinline__ void smith_pair(T sx, T sy, T sz, T cO, T cQ, T alpha
     const T y = sy + (T)s_real[4 * m + 1];
     const T z = sz + (T)s_real[4 * m + 2];
     const T l2 = x * x + y * y + z * z;
-    const T l = d_sqrt(l2);
-    const T il = (T)1 / l;
-    const T ec = d_erfc(alpha * l);
-    const T e = d_exp(-alpha2 * l2);
+    T l, il, ec, e, il2;
+    if constexpr (sizeof(T) == 4) {
+      // FP32: 1/l from the reciprocal square root, erfc from exp(-alpha^2 l^2)
+      // (erfc_as), 1/l^2 = (1/l)^2
+      asm("rsqrt.approx.f32 %0, %1;" : "=f"(il) : "f"(l2));
+      l = l2 * il;
+      e = __expf(-alpha2 * l2);
+      ec = erfc_as(alpha * l, e);
+      il2 = il * il;
+    } else {
+      l = d_sqrt(l2);
+      il = (T)1 / l;
+      ec = d_erfc(alpha * l);
+      e = d_exp(-alpha2 * l2);
+    }
     const T W = ec + q1 * alpha * l * e;
     const T il3 = il * il * il;
     add(d, comp[6], cO * ec * il + cQ * W * il3);
-    const T oc = (cO * (ec * il + o_real * e) - cQ * ((T)3 * W * il3 + q2 * e)) / l2;
+    const T num = cO * (ec * il + o_real * e) - cQ * ((T)3 * W * il3 + q2 * e);
+    T oc;
+    if constexpr (sizeof(T) == 4) oc = num * il2;
+    else oc = num / l2;
     add(acc[0], comp[0], oc * x * x);
     add(acc[1], comp[1], oc * y * y);
     add(acc[2], comp[2], oc * z * z);
