@@ -421,6 +421,17 @@ PBG_API int pbg_batch_set_schedule(pbg_batch *b, int merge_order, int ctas_per_s
  * receives the mean time of each candidate, merge order major
  * (2 * PBG_MERGE_ORDERS entries; -1 for a candidate not run). */
 PBG_API int pbg_batch_autotune(pbg_batch *b, int reps, int *best, float *ms, void *stream);
+/* One replica's factorisation task list (host only, no device needed; no
+ * counterpart in the reference): for an nt x nt tile grid in the batch's
+ * precision, tasks[4 t .. 4 t + 3] = (kind, i, j, k) of task t (cap tasks at
+ * most) and seg[s] the start of segment s (the last entry is the end; seg_cap
+ * entries at most).  The mixed list is left-looking (kinds 0 diagonal pair,
+ * 1 update pair, 2 solve pair; rows i and i + 1 of column j), the FP64 list
+ * right-looking (kinds 0 F, 1 S, 2 U, 4 U of rows i and i + 1; panel k).
+ * *n_tasks and *n_segs receive the counts; PBG_ERR_ARG if either does not
+ * fit or nt < 1. */
+PBG_API int pbg_cholesky_task_list(int nt, int precision, int *tasks, int cap, int *seg, int seg_cap,
+                                   int *n_tasks, int *n_segs);
 /* How the start of a step (Ewald build, copy into B, factorisation,
  * deterministic move) -- or with pbg_batch_step the whole step -- runs:
  * 1 = one CUDA graph launch (captured once a step

@@ -743,6 +743,25 @@ PBG_API int pbg_batch_destroy(pbg_batch* b) {
   return PBG_OK;
 }
 
+PBG_API int pbg_cholesky_task_list(int nt, int precision, int* tasks, int cap, int* seg, int seg_cap, int* n_tasks,
+                                   int* n_segs) {
+  if (nt < 1 || !tasks || !seg || !n_tasks || !n_segs) return PBG_ERR_ARG;
+  std::vector<int4> list;
+  std::vector<int> starts;
+  cholesky_replica_tasks(nt, precision, list, starts);
+  *n_tasks = (int)list.size();
+  *n_segs = (int)starts.size();
+  if ((int)list.size() > cap || (int)starts.size() > seg_cap) return PBG_ERR_ARG;
+  for (size_t t = 0; t < list.size(); ++t) {
+    tasks[4 * t + 0] = list[t].x;
+    tasks[4 * t + 1] = list[t].y;
+    tasks[4 * t + 2] = list[t].z;
+    tasks[4 * t + 3] = list[t].w;
+  }
+  for (size_t q = 0; q < starts.size(); ++q) seg[q] = starts[q];
+  return PBG_OK;
+}
+
 // Device bytes a replica of n_beads takes in a batch of this precision.
 PBG_API long long pbg_batch_footprint(int precision, int hydrodynamics, int ewald_imag, int n_beads) {
   const long long n = 3LL * n_beads, ld = (n + PBG_TILE - 1) / PBG_TILE * PBG_TILE, nt = ld / PBG_TILE;
