@@ -2795,6 +2795,163 @@ __global__ void b_invdiag_kernel(const T* __restrict__ G, int ld, int nt, T inv_
   }
 }
 
+// ---------------------------------------------------------------- X^T X on tcgen05 (FP32)
+// out = scale X^T X for the lower-triangular FP32 X (the SPD inverse's
+// symmetric product in the mixed lubricated path): a CTA forms the output
+// tiles (I, J) and (I + 1, J) (only (I, J) when I + 1 = nt) as one M = 128,
+// N = 64 product over the K range k = I .. nt-1,
+//   [X_kI^T; X_{k,I+1}^T] X_kJ    (X_{I,I+1} above the diagonal taken as 0),
+// in 3xTF32 on the tensor cores.  Per K-step the three tiles arrive row-major
+// by cp.async two K-steps ahead (raw stages); the transposition is done by
+// the split into the K-major hi / lo operands (column m of X_kI becomes row
+// m of A).  The accumulator restarts in TMEM every SYM_CHUNK K-steps and the
+// chunk sums are added in FP32 (as in the left-looking batch kernel).
+// Each element is written once: (r, c) and, off the diagonal tiles, (c, r);
+// with `reversed`, (ld-1-r, ld-1-c) instead.
+constexpr int SYM_CHUNK = 4;
+constexpr uint32_t SYM_SHARED_OFFSET = LL_OPERAND_BYTES + 2 * LL_RAW_BYTES;
+constexpr size_t sym_smem_bytes() { return SYM_SHARED_OFFSET + 16; }  // mbarrier, TMEM address
+static_assert(sym_smem_bytes() <= 227 * 1024, "the symmetric product does not fit an SM");
+
+// Output tile pairs: for each J, I = J, J + 2, J + 4, ...
+__host__ __device__ inline int sym_pairs(int nt) {
+  int n = 0;
+  for (int J = 0; J < nt; ++J) n += (nt - J + 1) / 2;
+  return n;
+}
+
+// The K-step k tiles: X_kI, X_{k,I+1} (when it is a lower tile), X_kJ.
+__device__ __forceinline__ void sym_fetch_step(const float* X, int ld, int I, int J, int k, bool two, float* raw) {
+  const float* row = X + (size_t)k * NB * ld;
+  ll_fetch_tile(row + (size_t)I * NB, ld, raw);
+  if (two && k >= I + 1) ll_fetch_tile(row + (size_t)(I + 1) * NB, ld, raw + NB * NB);
+  ll_fetch_tile(row + (size_t)J * NB, ld, raw + 2 * NB * NB);
+  cp_async_commit();
+}
+
+__global__ void __launch_bounds__(THREADS, 1) sym_tc_kernel(const float* __restrict__ X, int ld, int nt, float scale,
+                                                           int reversed, float* __restrict__ out, int* info) {
+  extern __shared__ __align__(1024) unsigned char sym_smem[];
+  unsigned char* base = sym_smem;
+  const int tid = threadIdx.x;
+  if (tc::smem_u32(base) & 1023u) {  // the operands need a 1024-byte aligned start
+    if (tid == 0) atomicCAS(info, 0, -1);
+    return;
+  }
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(base + SYM_SHARED_OFFSET);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(base + SYM_SHARED_OFFSET + 8);
+  int b = blockIdx.x, J = 0;
+  for (; J < nt; ++J) {
+    const int cnt = (nt - J + 1) / 2;
+    if (b < cnt) break;
+    b -= cnt;
+  }
+  const int I = J + 2 * b;
+  const bool two = I + 1 < nt;
+  if (tid == 0) tc::mbar_init(mbar, 1);
+  if (tid < 32) tc::tmem_alloc(s_tmem, 64);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *s_tmem;
+  uint32_t phase = 0;
+  unsigned char* Ahi = base;
+  unsigned char* Alo = Ahi + LL_A_BYTES;
+  unsigned char* Bhi = Alo + LL_A_BYTES;
+  unsigned char* Blo = Bhi + LL_B_BYTES;
+  float* raw[2] = {reinterpret_cast<float*>(base + LL_OPERAND_BYTES),
+                   reinterpret_cast<float*>(base + LL_OPERAND_BYTES + LL_RAW_BYTES)};
+  const int warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
+  const uint32_t tacc = tmem + ((uint32_t)(32 * q) << 16) + 32 * g;
+  // this thread's operand rows: A row ma (chunks 2e + tid / 128), B row nb
+  // (chunks 4e + tid / 64)
+  const int ma = tid & 127, nb = tid & 63;
+  sym_fetch_step(X, ld, I, J, I, two, raw[0]);
+  if (I + 1 < nt) sym_fetch_step(X, ld, I, J, I + 1, two, raw[1]);
+  float racc[32];
+#pragma unroll
+  for (int u = 0; u < 32; ++u) racc[u] = 0.0f;
+  bool ok = true;
+  for (int k = I; k < nt; ++k) {
+    const int s = k - I;
+    float* st = raw[s & 1];
+    if (k + 1 < nt) cp_async_wait_group<1>();
+    else cp_async_wait_group<0>();
+    __syncthreads();  // every thread's copies of this K-step are in
+    if (s > 0) {      // the products of the previous K-step have read the operands
+      if (!tc::mbar_wait(mbar, phase, SPIN_LIMIT)) ok = false;
+      phase ^= 1;
+      tc::fence_after_sync();
+      if (s % SYM_CHUNK == 0) {
+        float v[32];
+        tc::tmem_ld32(tacc, v);
+#pragma unroll
+        for (int u = 0; u < 32; ++u) racc[u] += v[u];
+        tc::fence_before_sync();
+      }
+    }
+    // A row ma: column ma of X_kI (ma < 64) or of X_{k,I+1} (zero for k = I
+    // or beyond the last tile); chunk c holds K = 4c .. 4c+3 (rows of X)
+    {
+      const bool zero = ma >= 64 && !(two && k >= I + 1);
+      const float* src = st + (ma < 64 ? 0 : NB * NB) + (ma & 63);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int c = 2 * e + (tid >> 7);
+        float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!zero) x = make_float4(src[(4 * c) * NB], src[(4 * c + 1) * NB], src[(4 * c + 2) * NB], src[(4 * c + 3) * NB]);
+        tc::store_split_chunk(x, tc::sw128_offset(128, ma, c), Ahi, Alo);
+      }
+      const float* srcb = st + 2 * NB * NB + nb;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int c = 4 * e + (tid >> 6);
+        const float4 x =
+            make_float4(srcb[(4 * c) * NB], srcb[(4 * c + 1) * NB], srcb[(4 * c + 2) * NB], srcb[(4 * c + 3) * NB]);
+        tc::store_split_chunk(x, tc::sw128_offset(64, nb, c), Bhi, Blo);
+      }
+    }
+    tc::fence_proxy_smem();
+    __syncthreads();  // operands written; every thread is past its reads of this stage
+    if (tid == 0) {
+      tc::fence_after_sync();
+      tc::issue_product(tmem, tc::smem_u32(Ahi), tc::smem_u32(Alo), tc::smem_u32(Bhi), tc::smem_u32(Blo),
+                        s % SYM_CHUNK != 0 ? 1u : 0u);
+      tc::mma_commit(mbar);
+    }
+    if (k + 2 < nt) sym_fetch_step(X, ld, I, J, k + 2, two, st);
+  }
+  if (!tc::mbar_wait(mbar, phase, SPIN_LIMIT)) ok = false;
+  ok = __syncthreads_and(ok) != 0;
+  tc::fence_after_sync();
+  {
+    float v[32];
+    tc::tmem_ld32(tacc, v);
+#pragma unroll
+    for (int u = 0; u < 32; ++u) racc[u] += v[u];
+  }
+  const int m = 32 * q + lane, t = m >> 6;
+  if (ok && (t == 0 || two)) {
+    const int It = I + t;
+    const int r0 = It * NB + (m & 63), c0 = J * NB + 32 * g;
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      const float v = racc[u] * scale;
+      int r = r0, c = c0 + u;
+      if (reversed) {
+        r = ld - 1 - r;
+        c = ld - 1 - c;
+      }
+      out[(size_t)r * ld + c] = v;
+      if (It != J) out[(size_t)c * ld + r] = v;
+    }
+  }
+  if (!ok && tid == 0) atomicCAS(info, 0, -1);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) tc::tmem_dealloc(tmem, 64);
+}
+
 // Dynamic shared memory above the 48 KB default (the FP64 tiles), set on the
 // current device before each use.
 template <typename T>
@@ -2864,8 +3021,14 @@ int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st) {
   return launch_trtri_diag(w.invdiag, w.X, ld, PBG_PREC_MIXED, st);
 }
 
-int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, cudaStream_t st) {
-  return lauum_tc<float>(X, ld, scale, reversed, out, st);
+int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, int* info, cudaStream_t st) {
+  if (ld % NB != 0 || ld <= 0) return PBG_ERR_ARG;
+  const int nt = ld / NB;
+  PBG_CUDA_TRY(cudaFuncSetAttribute(sym_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sym_smem_bytes()));
+  sym_tc_kernel<<<sym_pairs(nt), THREADS, sym_smem_bytes(), st>>>(X, ld, nt, scale, reversed ? 1 : 0, out, info);
+  PBG_CHECK_LAUNCH();
+  return PBG_OK;
 }
 
 int tc_reversed_factor(const float* X, const float* G, int ld, double s, float* B, float* invdiag,

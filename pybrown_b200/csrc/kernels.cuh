@@ -142,7 +142,8 @@ int launch_trtri_diag(const void* invdiag, void* X, int ld, int precision, cudaS
 int launch_lauum_tc(const void* X, int ld, double scale, bool reversed, void* out, int precision, cudaStream_t st);
 // SPD inverse of the mixed lubricated path (FP32).  The caller puts the
 // matrix (order ld, padded) in F; tc_factor_invert factors it in place
-// (F = G, lower) and forms X = inv(G); tc_lauum writes scale X^T X;
+// (F = G, lower) and forms X = inv(G); tc_lauum writes scale X^T X on the
+// tcgen05 tensor cores (a wait that gives up sets *info = -1);
 // tc_reversed_factor writes B = s J X^T J (lower; J reverses all ld indices)
 // and the inverted diagonal tiles of that B, for launch_trsv_upper.
 struct TcInverseWork {
@@ -154,7 +155,7 @@ struct TcInverseWork {
 size_t tc_inverse_work_bytes(int ld);
 TcInverseWork tc_inverse_work(void* work, int ld);
 int tc_factor_invert(int ld, int* info, void* work, cudaStream_t st);
-int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, cudaStream_t st);
+int tc_lauum(const float* X, int ld, float scale, bool reversed, float* out, int* info, cudaStream_t st);
 int tc_reversed_factor(const float* X, const float* G, int ld, double s, float* B, float* invdiag,
                        cudaStream_t st);
 

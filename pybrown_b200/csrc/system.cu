@@ -326,7 +326,7 @@ int compute_Dff(pbg_system* s, cudaStream_t st, bool fill_B) {
     PBG_CUDA_TRY(cudaMemcpyAsync(w.F, s->Mff, (size_t)s->ld * s->ld * sizeof(float), cudaMemcpyDeviceToDevice, st));
     s->work_holds_R = false;
     if ((rc = tc_factor_invert(s->ld, s->dflags + 2, s->inv_work, st))) return rc;
-    return tc_lauum(w.X, s->ld, 1.0f, false, (float*)s->Rff, st);
+    return tc_lauum(w.X, s->ld, 1.0f, false, (float*)s->Rff, s->dflags + 2, st);
   }
   rc = launch_rpy_tensor(src, s->pos, s->radii, smith, s->tables, scale, PBG_PREC_FP64, s->Mff, s->ld, s->phase, st);
   if (rc) return rc;
@@ -361,7 +361,7 @@ int compute_Dtot(pbg_system* s, cudaStream_t st) {
     if (rc) return rc;
     if ((rc = factor_reversed_R(s, s->dflags + 3, st))) return rc;
     const TcInverseWork w = tc_inverse_work(s->inv_work, s->ld);
-    return tc_lauum(w.X, s->ld, (float)p.kBT, true, (float*)s->D, st);
+    return tc_lauum(w.X, s->ld, (float)p.kBT, true, (float*)s->D, s->dflags + 3, st);
   }
   const size_t bytes = (size_t)s->ld * s->ld * sizeof(double);
   PBG_CUDA_TRY(cudaMemcpyAsync(s->R, s->Rff, bytes, cudaMemcpyDeviceToDevice, st));

@@ -180,6 +180,20 @@ __device__ __forceinline__ void store_share_split(const TileShare<NTHREADS>& s, 
   }
 }
 
+// Writes the hi / lo TF32 halves of four FP32 values (one 16-byte chunk) at
+// byte offset off of the hi and lo operands.
+__device__ __forceinline__ void store_split_chunk(float4 x4, uint32_t off, unsigned char* hi, unsigned char* lo) {
+  const float x[4] = {x4.x, x4.y, x4.z, x4.w};
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    h[u] = rna_tf32(x[u]);
+    l[u] = rna_tf32(x[u] - __uint_as_float(h[u]));
+  }
+  *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
 // Loads up to MAXT 64 x 64 FP32 tiles (row stride ld) and writes their hi /
 // lo TF32 halves into the operands: every thread issues all of its loads
 // (16 bytes each, through L2) before the first conversion, so the tiles cost
